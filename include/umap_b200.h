@@ -1,0 +1,140 @@
+/*
+ * libumap_b200 — C ABI of the B200 (sm_100a) UMAP hot path.
+ *
+ * The reference (hanxiao/mlx-vis 0.7.0) has no FFI: its hot path is Python
+ * calling MLX built-ins.  Each entry point below replaces one reference call
+ * site, cited as file:line relative to the reference checkout.
+ *
+ * Conventions
+ *  - Every function returns an int status (UMAPB_OK == 0).  On failure
+ *    umapb_last_error() returns a message for the calling thread.
+ *  - Array arguments are DEVICE pointers, row-major, caller-owned.  The library
+ *    allocates no device memory: functions that need scratch take a caller-owned
+ *    workspace whose size the matching *_workspace query returns.
+ *  - All work is enqueued on `stream` (a cudaStream_t; NULL = legacy default).
+ *    Calls are asynchronous; results are valid once the stream is synchronised.
+ *  - Kernels with device-side waits bound every wait in time.  If one expires
+ *    the kernel abandons its work and writes a non-zero code into the int32
+ *    device status word at the start of the workspace; umapb_read_status()
+ *    copies it back (synchronising the stream) and turns it into a status.
+ */
+#ifndef UMAP_B200_H_
+#define UMAP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UMAPB_OK 0
+#define UMAPB_ERR_ARG 1          /* invalid argument (shape, k, null pointer, ...) */
+#define UMAPB_ERR_UNSUPPORTED 2  /* valid request outside the implemented envelope */
+#define UMAPB_ERR_CUDA 3         /* CUDA runtime/driver error (launch, encode, ...) */
+#define UMAPB_ERR_WORKSPACE 4    /* workspace null or smaller than the query said */
+#define UMAPB_ERR_DEVICE 5       /* a kernel reported a device-side failure (bounded wait expired) */
+
+typedef struct CUstream_st* umapb_stream_t;
+
+/* Message for the last failed call on this thread ("" if none). */
+const char* umapb_last_error(void);
+/* ABI version of this library. */
+int umapb_abi_version(void);
+/* Synchronises `stream`, reads the device status word at `workspace` and
+ * returns UMAPB_OK or UMAPB_ERR_DEVICE (with a message). */
+int umapb_read_status(const void* workspace, umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Exact brute-force kNN — replaces mlx_vis/_knn.py:47-88 (chunked
+ * |x|^2+|y|^2-2x.y GEMM, self += 1e30, full-row argsort, first k, sqrt).
+ * BF16 tcgen05 distance tiles with a fused per-row top-(k+extra) selection,
+ * then an exact FP32 rerank of those candidates.
+ *   X        (n, d) float32
+ *   out_idx  (n, k) int32   ascending distance, self excluded
+ *   out_dist (n, k) float32 Euclidean (squared != 0: squared distances)
+ * Requires 1 <= k <= n-1 and k + extra <= 128.
+ * ------------------------------------------------------------------------- */
+int umapb_knn_brute_workspace(int64_t n, int64_t d, int32_t k, int32_t extra, size_t* bytes);
+int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                    int32_t* out_idx, float* out_dist, void* workspace, size_t workspace_bytes,
+                    umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Fuzzy simplicial set — replaces UMAP._fuzzy_simplicial_set
+ * (mlx_vis/_umap/umap.py:199-270, with _searchsorted 8-22).
+ * Per-row rho and sigma bisection (64 steps, target log2 k, tolerance 1e-5) in
+ * FP64 (fp64_bisection != 0) or FP32 (the reference's precision); weights
+ * exp(-max(d-rho,0)/max(sigma,1e-10)); symmetrisation w + w' - w*w' over the
+ * n*k directed edges; prune w < max(w)/n_epochs keeping row-major order.
+ *   knn_idx (n, k) int32, knn_dist (n, k) float32 (Euclidean, ascending)
+ *   rows/cols/vals: capacity n*k; *n_edges (device int64) receives the count.
+ *   rho_out, sigma_out: optional (n,) float32 (may be NULL).
+ * ------------------------------------------------------------------------- */
+int umapb_fuzzy_workspace(int64_t n, int32_t k, size_t* bytes);
+int umapb_fuzzy(const int32_t* knn_idx, const float* knn_dist, int64_t n, int32_t k, int32_t n_epochs,
+                int32_t fp64_bisection, int32_t* rows, int32_t* cols, float* vals, int64_t* n_edges,
+                float* rho_out, float* sigma_out, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Spectral initialisation — replaces UMAP._spectral_init power iteration
+ * (mlx_vis/_umap/umap.py:298-348).  Graph in row-major edge order (as
+ * umapb_fuzzy writes it), `n_edges` a device int64, `e_cap` its capacity.
+ *   V0    (n, dim+1) float32 start block (the reference draws it from mx.random)
+ *   noise (n, dim)   float32 N(0, 1e-4) draw added after the 10/max|e| scaling
+ *   Y     (n, dim)   float32 output, min-max scaled to [0, 10] per column
+ * Each power iteration is one CSR SpMV that also accumulates the FP64 Gram
+ * matrix; orthonormalisation uses its Cholesky factor (the same Q as the
+ * reference's modified Gram-Schmidt).
+ * ------------------------------------------------------------------------- */
+/* Standard normal draws for the spectral start block V0 — stands in for
+ * mx.random.normal((n, c+1)) after mx.random.seed (umap.py:134-135, 325),
+ * whose bit stream MLX does not specify: Philox4x32-10 + Box-Muller. */
+int umapb_normal_fill(float* out, int64_t count, uint64_t seed, umapb_stream_t stream);
+int umapb_spectral_workspace(int64_t n, int32_t dim, int64_t e_cap, int32_t n_iter, size_t* bytes);
+int umapb_spectral(const int32_t* rows, const int32_t* cols, const float* vals, const int64_t* n_edges,
+                   int64_t e_cap, int64_t n, int32_t dim, const float* V0, int32_t n_iter, const float* noise,
+                   float* Y, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Layout optimisation — replaces UMAP._optimize / _sgd_step
+ * (mlx_vis/_umap/umap.py:359-449).
+ * umapb_layout_prepare: epochs_per_sample = n_epochs / (n_epochs * w/max w)
+ *   in float32 (umap.py:398-403) into eps[e_cap]; next[e] = eps[e].
+ * umapb_layout_epochs: runs epochs [epoch_begin, epoch_end).  An edge is active
+ *   in an epoch when next <= epoch (then next += eps, float32), exactly the
+ *   reference's host schedule.  Each epoch reads the epoch-start Y and
+ *   accumulates all moves before applying them (the reference's synchronous
+ *   scatter-add semantics).  Negative tails come from a counter-based Philox
+ *   stream keyed by (seed, epoch, edge, sample).
+ * umapb_layout_epoch_injected: one epoch whose negative tails are given in the
+ *   reference's order (sample j pairs head ef[j % A] with neg_to[j], A = number
+ *   of active edges, umap.py:433-436); neg_count must equal neg_rate * A.
+ * Y (n, dim) float32 is updated in place; dim in {1, 2, 3, 4}.
+ * ------------------------------------------------------------------------- */
+int umapb_layout_workspace(int64_t n, int32_t dim, int64_t e_cap, size_t* bytes);
+int umapb_layout_prepare(const float* vals, const int64_t* n_edges, int64_t e_cap, int32_t n_epochs, float* eps,
+                         float* next, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
+int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                        const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int32_t epoch_begin,
+                        int32_t epoch_end, int32_t n_epochs, float a, float b, float learning_rate,
+                        int32_t neg_rate, uint64_t seed, void* workspace, size_t workspace_bytes,
+                        umapb_stream_t stream);
+/* Number of edges active in `epoch` given the current `next` values (written to
+ * the device int64 *count) — the emptiness test of umap.py:409-414/424 that
+ * decides whether the reference runs an epoch and calls epoch_callback.  Uses
+ * the layout workspace. */
+int umapb_layout_count_active(const float* next, const int64_t* n_edges, int64_t n, int32_t dim, int64_t e_cap,
+                              int32_t epoch, int64_t* count, void* workspace, size_t workspace_bytes,
+                              umapb_stream_t stream);
+int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                                const float* eps, float* next, const int64_t* n_edges, int64_t e_cap,
+                                int32_t epoch, int32_t n_epochs, float a, float b, float learning_rate,
+                                int32_t neg_rate, const int32_t* neg_to, int64_t neg_count, void* workspace,
+                                size_t workspace_bytes, umapb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UMAP_B200_H_ */

@@ -1,0 +1,230 @@
+"""ctypes binding of libumap_b200.so (declared in include/umap_b200.h).
+
+PyTorch provides device memory and streams; every compute step is a kernel of
+libumap_b200.  There is no fallback: if the library is missing or a call fails,
+an exception is raised.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libumap_b200.so")
+
+_c = ctypes
+_i32, _i64, _u64, _f32, _sz = _c.c_int32, _c.c_int64, _c.c_uint64, _c.c_float, _c.c_size_t
+_p = _c.c_void_p
+_psz = _c.POINTER(_c.c_size_t)
+
+# name -> argtypes (all functions return int status unless listed in _RESTYPES)
+SIGNATURES = {
+    "umapb_last_error": [],
+    "umapb_abi_version": [],
+    "umapb_read_status": [_p, _p],
+    "umapb_knn_brute_workspace": [_i64, _i64, _i32, _i32, _psz],
+    "umapb_knn_brute": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _sz, _p],
+    "umapb_fuzzy_workspace": [_i64, _i32, _psz],
+    "umapb_fuzzy": [_p, _p, _i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
+    "umapb_normal_fill": [_p, _i64, _u64, _p],
+    "umapb_spectral_workspace": [_i64, _i32, _i64, _i32, _psz],
+    "umapb_spectral": [_p, _p, _p, _p, _i64, _i64, _i32, _p, _i32, _p, _p, _p, _sz, _p],
+    "umapb_layout_workspace": [_i64, _i32, _i64, _psz],
+    "umapb_layout_prepare": [_p, _p, _i64, _i32, _p, _p, _p, _sz, _p],
+    "umapb_layout_epochs": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32,
+                            _u64, _p, _sz, _p],
+    "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
+    "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
+                                    _p, _i64, _p, _sz, _p],
+}
+_RESTYPES = {"umapb_last_error": _c.c_char_p}
+
+_lock = threading.Lock()
+_lib = None
+
+
+class UmapB200Error(RuntimeError):
+    """A libumap_b200 call returned a non-zero status."""
+
+    def __init__(self, func: str, status: int, message: str):
+        super().__init__(f"{func} failed with status {status}: {message}")
+        self.func = func
+        self.status = status
+
+
+def load() -> ctypes.CDLL:
+    """Loads the library once and declares every signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m mlx_vis_b200.build` "
+                                   "(the CUDA kernels are required; there is no CPU fallback)")
+            lib = ctypes.CDLL(LIB_PATH)
+            for name, argtypes in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = argtypes
+                fn.restype = _RESTYPES.get(name, _c.c_int)
+            _lib = lib
+    return _lib
+
+
+def call(name: str, *args) -> None:
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != 0:
+        msg = lib.umapb_last_error().decode(errors="replace")
+        raise UmapB200Error(name, status, msg)
+
+
+def query(name: str, *args) -> int:
+    out = ctypes.c_size_t(0)
+    call(name, *args, ctypes.byref(out))
+    return int(out.value)
+
+
+def ptr(t) -> ctypes.c_void_p:
+    if t is None:
+        return ctypes.c_void_p(0)
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def stream_handle(stream=None) -> ctypes.c_void_p:
+    s = torch.cuda.current_stream() if stream is None else stream
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def workspace(nbytes: int, device) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def read_status(ws: torch.Tensor, stream=None) -> None:
+    """Synchronises the stream and raises if a kernel reported a device-side failure."""
+    call("umapb_read_status", ptr(ws), stream_handle(stream))
+
+
+# ---------------------------------------------------------------------------
+# thin typed wrappers over the C ABI (device tensors in, device tensors out)
+# ---------------------------------------------------------------------------
+
+def _require(t: torch.Tensor, dtype, ndim=None, name="tensor"):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if ndim is not None and t.dim() != ndim:
+        raise ValueError(f"{name} must have {ndim} dimensions")
+    return t.contiguous()
+
+
+def knn_brute(X: torch.Tensor, k: int, extra: int = 16, squared: bool = False, check: bool = True):
+    """Exact kNN of the rows of X (n, d) float32: (idx int32 (n,k), dist float32 (n,k))."""
+    X = _require(X, torch.float32, 2, "X")
+    n, d = X.shape
+    nbytes = query("umapb_knn_brute_workspace", n, d, k, extra)
+    ws = workspace(nbytes, X.device)
+    idx = torch.empty((n, k), dtype=torch.int32, device=X.device)
+    dist = torch.empty((n, k), dtype=torch.float32, device=X.device)
+    call("umapb_knn_brute", ptr(X), n, d, k, extra, int(squared), ptr(idx), ptr(dist), ptr(ws), ws.numel(),
+         stream_handle())
+    if check:
+        read_status(ws)
+    return idx, dist
+
+
+def fuzzy(knn_idx: torch.Tensor, knn_dist: torch.Tensor, n_epochs: int, fp64: bool = True,
+          with_sigma: bool = False):
+    """Fuzzy simplicial set: (rows, cols, vals, n_edges) with capacity n*k; n_edges is a
+    device int64 tensor of shape (1,).  With ``with_sigma`` also returns (rho, sigma)."""
+    knn_idx = _require(knn_idx, torch.int32, 2, "knn_idx")
+    knn_dist = _require(knn_dist, torch.float32, 2, "knn_dist")
+    n, k = knn_idx.shape
+    dev = knn_idx.device
+    ws = workspace(query("umapb_fuzzy_workspace", n, k), dev)
+    rows = torch.empty(n * k, dtype=torch.int32, device=dev)
+    cols = torch.empty(n * k, dtype=torch.int32, device=dev)
+    vals = torch.empty(n * k, dtype=torch.float32, device=dev)
+    n_edges = torch.zeros(1, dtype=torch.int64, device=dev)
+    rho = torch.empty(n, dtype=torch.float32, device=dev) if with_sigma else None
+    sigma = torch.empty(n, dtype=torch.float32, device=dev) if with_sigma else None
+    call("umapb_fuzzy", ptr(knn_idx), ptr(knn_dist), n, k, int(n_epochs), int(bool(fp64)), ptr(rows), ptr(cols),
+         ptr(vals), ptr(n_edges), ptr(rho), ptr(sigma), ptr(ws), ws.numel(), stream_handle())
+    if with_sigma:
+        return rows, cols, vals, n_edges, rho, sigma
+    return rows, cols, vals, n_edges
+
+
+def normal(shape, seed: int, device) -> torch.Tensor:
+    """Standard normal float32 tensor drawn by the library's Philox kernel."""
+    out = torch.empty(shape, dtype=torch.float32, device=device)
+    call("umapb_normal_fill", ptr(out), out.numel(), int(seed) & 0xFFFFFFFFFFFFFFFF, stream_handle())
+    return out
+
+
+def spectral(rows, cols, vals, n_edges, n: int, dim: int, V0: torch.Tensor, noise: torch.Tensor,
+             n_iter: int = 100) -> torch.Tensor:
+    V0 = _require(V0, torch.float32, 2, "V0")
+    noise = _require(noise, torch.float32, 2, "noise")
+    dev = V0.device
+    e_cap = rows.numel()
+    ws = workspace(query("umapb_spectral_workspace", n, dim, e_cap, n_iter), dev)
+    Y = torch.empty((n, dim), dtype=torch.float32, device=dev)
+    call("umapb_spectral", ptr(rows), ptr(cols), ptr(vals), ptr(n_edges), e_cap, n, dim, ptr(V0), int(n_iter),
+         ptr(noise), ptr(Y), ptr(ws), ws.numel(), stream_handle())
+    return Y
+
+
+class Layout:
+    """Device state of one optimize_layout run (schedule + workspace)."""
+
+    def __init__(self, rows, cols, vals, n_edges, n: int, dim: int, n_epochs: int):
+        self.rows, self.cols, self.n_edges = rows, cols, n_edges
+        self.n, self.dim, self.n_epochs = int(n), int(dim), int(n_epochs)
+        self.e_cap = rows.numel()
+        dev = rows.device
+        self.ws = workspace(query("umapb_layout_workspace", self.n, self.dim, self.e_cap), dev)
+        self.eps = torch.empty(max(self.e_cap, 1), dtype=torch.float32, device=dev)
+        self.next = torch.empty(max(self.e_cap, 1), dtype=torch.float32, device=dev)
+        call("umapb_layout_prepare", ptr(vals), ptr(n_edges), self.e_cap, self.n_epochs, ptr(self.eps),
+             ptr(self.next), ptr(self.ws), self.ws.numel(), stream_handle())
+
+    def epochs(self, Y: torch.Tensor, begin: int, end: int, a: float, b: float, learning_rate: float,
+               neg_rate: int, seed: int):
+        call("umapb_layout_epochs", ptr(Y), self.n, self.dim, ptr(self.rows), ptr(self.cols), ptr(self.eps),
+             ptr(self.next), ptr(self.n_edges), self.e_cap, int(begin), int(end), self.n_epochs, float(a), float(b),
+             float(learning_rate), int(neg_rate), int(seed) & 0xFFFFFFFFFFFFFFFF, ptr(self.ws), self.ws.numel(),
+             stream_handle())
+
+    def count_active(self, epoch: int) -> int:
+        """Active edges in ``epoch`` for the current schedule state (synchronises)."""
+        out = torch.zeros(1, dtype=torch.int64, device=self.rows.device)
+        call("umapb_layout_count_active", ptr(self.next), ptr(self.n_edges), self.n, self.dim, self.e_cap,
+             int(epoch), ptr(out), ptr(self.ws), self.ws.numel(), stream_handle())
+        return int(out.item())
+
+    def epoch_injected(self, Y: torch.Tensor, epoch: int, a: float, b: float, learning_rate: float, neg_rate: int,
+                       neg_to: torch.Tensor):
+        neg_to = _require(neg_to, torch.int32, 1, "neg_to")
+        call("umapb_layout_epoch_injected", ptr(Y), self.n, self.dim, ptr(self.rows), ptr(self.cols),
+             ptr(self.eps), ptr(self.next), ptr(self.n_edges), self.e_cap, int(epoch), self.n_epochs, float(a),
+             float(b), float(learning_rate), int(neg_rate), ptr(neg_to), neg_to.numel(), ptr(self.ws),
+             self.ws.numel(), stream_handle())
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)
+
+
+def to_numpy(t: torch.Tensor) -> np.ndarray:
+    return t.detach().cpu().numpy()

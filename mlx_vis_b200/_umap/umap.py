@@ -1,0 +1,240 @@
+"""UMAP on one B200 — drop-in for ``mlx_vis.UMAP`` (mlx_vis/_umap/umap.py:25-449).
+
+Same constructor arguments and defaults (umap.py:46-60) and the same
+``fit_transform(X, epoch_callback=None)`` contract (umap.py:75-144): host float32
+result of shape (n, n_components), stored in ``embedding_``; ``n_epochs``
+defaults to 500 for n <= 10000 and 200 above and is written back to the
+estimator (umap.py:123-124); ``epoch_callback(epoch, Y)`` is called with epoch 0
+and after every epoch that has active edges (umap.py:420-442).
+
+Pipeline, all on the GPU through libumap_b200:
+  kNN (brute tcgen05 / NNDescent) -> fuzzy set (FP64 sigma bisection)
+  -> spectral init (CSR SpMV + Cholesky-QR power iteration)
+  -> layout epochs (exact float32 schedule, synchronous SGD), by default
+     recorded once into a CUDA graph and replayed.
+Host work left: the a/b curve fit (float64, microseconds) and the reference's
+NumPy noise draw for the spectral rescale (umap.py:344).
+
+New keyword arguments (defaults keep the reference behaviour):
+  init        "spectral" (reference), "random" (N(0, 1e-4) like the reference's
+              fallback), or "learned" (the MLP warm start of ``encoder``)
+  encoder     a trained ``mlx_vis_b200.encoder.Encoder`` for init="learned"
+  use_graph   capture the epoch loop in a CUDA graph (no callback only)
+"""
+
+from __future__ import annotations
+
+import os
+import time
+
+import numpy as np
+import torch
+
+from mlx_vis_b200 import _lib
+from mlx_vis_b200._curve import find_ab_params
+from mlx_vis_b200._device import device, to_device_f32, to_host
+from mlx_vis_b200._normalize import normalize_input
+
+
+def _random_seed() -> int:
+    return int.from_bytes(os.urandom(8), "little")
+
+
+class UMAP:
+    """UMAP dimensionality reduction on an NVIDIA B200.
+
+    Parameters mirror mlx_vis.UMAP: n_components, n_neighbors, min_dist, spread,
+    n_epochs, learning_rate, negative_sample_rate, random_state, verbose, pca_dim,
+    knn_method ("auto" | "brute" | "nndescent"), normalize.
+    """
+
+    def __init__(
+        self,
+        n_components: int = 2,
+        n_neighbors: int = 15,
+        min_dist: float = 0.1,
+        spread: float = 1.0,
+        n_epochs: int | None = None,
+        learning_rate: float = 1.0,
+        negative_sample_rate: int = 5,
+        random_state: int | None = None,
+        verbose: bool = False,
+        pca_dim: int | None = None,
+        knn_method: str = "auto",
+        normalize: str | bool = False,
+        init: str = "spectral",
+        encoder=None,
+        use_graph: bool = True,
+    ):
+        self.n_components = n_components
+        self.n_neighbors = n_neighbors
+        self.min_dist = min_dist
+        self.spread = spread
+        self.n_epochs = n_epochs
+        self.learning_rate = learning_rate
+        self.negative_sample_rate = negative_sample_rate
+        self.random_state = random_state
+        self.verbose = verbose
+        self.pca_dim = pca_dim
+        self.knn_method = knn_method
+        self.normalize = normalize
+        self.init = init
+        self.encoder = encoder
+        self.use_graph = use_graph
+        self.embedding_ = None
+        self.timings_ = {}
+        self.graph_ = None
+
+    # ------------------------------------------------------------------
+    def fit_transform(self, X, epoch_callback=None) -> np.ndarray:
+        """Fit UMAP and return the embedding (host float32, (n, n_components))."""
+        Y = self.fit_transform_device(X, epoch_callback=epoch_callback)
+        self.embedding_ = to_host(Y)
+        return self.embedding_
+
+    def fit_transform_device(self, X, epoch_callback=None) -> torch.Tensor:
+        """Like fit_transform but returns the CUDA tensor (no device-to-host copy)."""
+        if self.n_components < 1 or self.n_components > 4:
+            raise ValueError("n_components must be between 1 and 4")
+        dev = device()
+        ev = _Events(dev)
+        if self.normalize:
+            Xh = X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else np.asarray(X, dtype=np.float32)
+            X = normalize_input(np.asarray(Xh, dtype=np.float32), self.normalize).astype(np.float32)
+        Xd = to_device_f32(X, dev)
+        n, dim = Xd.shape
+        if n < 2:
+            raise ValueError("UMAP needs at least 2 samples")
+        ev.mark("upload")
+
+        if self.pca_dim is not None and dim > self.pca_dim:
+            Xd = self._pca(Xd)
+            ev.mark("pca")
+
+        if self.verbose:
+            print("Computing nearest neighbors...")
+        from mlx_vis_b200._knn import knn_device
+
+        k = min(self.n_neighbors, n - 1)
+        knn_idx, knn_dist = knn_device(Xd, k, method=self.knn_method, verbose=self.verbose,
+                                       random_state=self.random_state)
+        ev.mark("knn")
+
+        if self.n_epochs is None:
+            self.n_epochs = 500 if n <= 10000 else 200
+        if self.verbose:
+            print("Building fuzzy simplicial set...")
+        rows, cols, vals, n_edges = _lib.fuzzy(knn_idx, knn_dist, self.n_epochs, fp64=True)
+        ev.mark("fuzzy")
+
+        a, b = find_ab_params(self.spread, self.min_dist)
+        self.a_, self.b_ = a, b
+        seed = self.random_state if self.random_state is not None else _random_seed()
+
+        if self.verbose:
+            print("Initializing embedding...")
+        Y = self._init_embedding(Xd, rows, cols, vals, n_edges, n, seed)
+        ev.mark("init")
+
+        self._optimize(rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback)
+        ev.mark("layout")
+        self.timings_ = ev.finish()
+        self.graph_info_ = {"n_edges": int(n_edges.item())}
+        return Y
+
+    # ------------------------------------------------------------------
+    def _pca(self, Xd: torch.Tensor) -> torch.Tensor:
+        """Optional PCA (umap.py:92-111): covariance GEMM and eigh on the device."""
+        n = Xd.shape[0]
+        mean = Xd.mean(dim=0)
+        Xc = Xd - mean
+        cov = (Xc.T @ Xc) / (n - 1)
+        evals, evecs = torch.linalg.eigh(cov.double())
+        proj = evecs[:, -self.pca_dim:].flip(-1).float()
+        if self.verbose:
+            ret = float(evals[-self.pca_dim:].sum() / evals.sum())
+            print(f"Variance retained: {ret * 100:.1f}%")
+        return (Xc @ proj).contiguous()
+
+    def _init_embedding(self, Xd, rows, cols, vals, n_edges, n, seed) -> torch.Tensor:
+        c = self.n_components
+        dev = Xd.device
+        if self.init == "learned":
+            if self.encoder is None:
+                raise ValueError("init='learned' needs an encoder")
+            return self.encoder.init_layout(Xd)
+        if self.init == "random":
+            return _lib.normal((n, c), seed, dev) * 0.01
+        if self.init != "spectral":
+            raise ValueError(f"unknown init {self.init!r}")
+        try:
+            V0 = _lib.normal((n, c + 1), seed, dev)
+            rng = np.random.RandomState(self.random_state or 42)
+            noise = rng.normal(scale=0.0001, size=(n, c)).astype(np.float32)
+            noise_d = torch.from_numpy(noise).to(dev, non_blocking=True)
+            Y = _lib.spectral(rows, cols, vals, n_edges, n, c, V0, noise_d, n_iter=100)
+            if self.verbose:
+                print("Using spectral initialization")
+            return Y
+        except _lib.UmapB200Error as e:  # the reference falls back to random init (umap.py:354-357)
+            if self.verbose:
+                print(f"Spectral init failed ({e}), using random initialization")
+            return _lib.normal((n, c), seed, dev) * 0.01
+
+    def _optimize(self, rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback):
+        ne = int(self.n_epochs)
+        lay = _lib.Layout(rows, cols, vals, n_edges, n, self.n_components, ne)
+        layout_seed = (seed * 0x9E3779B97F4A7C15 + 1) & 0xFFFFFFFFFFFFFFFF
+        args = (a, b, self.learning_rate, self.negative_sample_rate, layout_seed)
+        if epoch_callback is not None:
+            epoch_callback(0, to_host(Y))
+            for e in range(ne):
+                if lay.count_active(e) == 0:
+                    continue
+                lay.epochs(Y, e, e + 1, *args)
+                epoch_callback(e + 1, to_host(Y))
+                if self.verbose and (e + 1) % 50 == 0:
+                    print(f"Epoch {e + 1}/{ne}")
+            return
+        if self.use_graph and ne > 0:
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                g.capture_begin()
+                lay.epochs(Y, 0, ne, *args)
+                g.capture_end()
+            torch.cuda.current_stream().wait_stream(s)
+            g.replay()
+            self.graph_ = g  # keep the graph alive until its work has finished
+        else:
+            lay.epochs(Y, 0, ne, *args)
+        if self.verbose:
+            print(f"Epoch {ne}/{ne}")
+
+
+class _Events:
+    """Per-stage CUDA-event timings (milliseconds) collected without extra syncs."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.t0 = time.perf_counter()
+        self.start = torch.cuda.Event(enable_timing=True)
+        self.start.record()
+        self.marks = []
+
+    def mark(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        self.marks.append((name, e))
+
+    def finish(self):
+        torch.cuda.synchronize(self.dev)
+        out = {}
+        prev = self.start
+        for name, e in self.marks:
+            out[name] = prev.elapsed_time(e)
+            prev = e
+        out["total_device"] = self.start.elapsed_time(prev)
+        out["total_wall"] = (time.perf_counter() - self.t0) * 1000.0
+        return out

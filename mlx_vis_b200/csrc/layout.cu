@@ -1,0 +1,443 @@
+// Layout optimisation — replaces UMAP._optimize and UMAP._sgd_step,
+// mlx_vis/_umap/umap.py:359-449.
+//
+// Schedule (umap.py:398-414): eps_e = n_epochs / (n_epochs * (w_e / max w)) in
+// float32, next_e starts at eps_e; edge e is active in epoch t when
+// next_e <= t, after which next_e += eps_e (float32).  The reference builds all
+// active sets on the host up front; here every epoch kernel re-evaluates the
+// same float32 recurrence per edge, so the sets are identical and no host work
+// or per-epoch index list is needed.
+//
+// Epoch (umap.py:359-387): every gather reads the epoch-start Y; the moves of
+// all pairs are accumulated into dY with float atomics and applied by a second
+// kernel, which reproduces the reference's synchronous scatter-add semantics.
+// Per active edge (i, j): attractive move clip(-2ab d^{2(b-1)}/(1+a d^{2b}) diff,
+// +-4) * alpha added to i and subtracted from j; neg_rate negatives (i, t) each
+// add clip(2b/((0.001+d^2)(1+a d^{2b})) diff, +-4) * alpha to i only.  The moves
+// of one edge on its head are summed in registers before one atomic.
+//
+// Negatives: the reference pairs sample s of an epoch with head ef[s % A] and a
+// uniform tail from mx.random.randint (umap.py:433-436).  The fast path draws
+// the tail of (epoch, edge e, sample m) from Philox4x32-10 (Salmon et al., SC'11)
+// keyed by the seed, mapped to [0, n) by a 32x32->64 multiply-high (bias below
+// n / 2^32).  The injected path takes the reference's own tails: it ranks the
+// active edges in edge order (block counts + scan) and uses tail neg_to[r + m A]
+// for the r-th active edge.
+#include <math.h>
+
+#include "common.cuh"
+#include "philox.cuh"
+#include "scan.cuh"
+
+namespace umapb {
+namespace layout {
+
+constexpr int kBlock = 256;
+constexpr int kEdgesPerBlock = 1024;
+
+// ---- reference pair math (float32, evaluation order of umap.py:361-383) ----
+struct Params {
+  float a, b, bm1, two_b, alpha;
+};
+
+template <int DIM>
+__device__ __forceinline__ void attract(const float (&yi)[DIM], const float (&yj)[DIM], const Params& p,
+                                        float (&out)[DIM]) {
+  float diff[DIM];
+  float d2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    diff[c] = __fsub_rn(yi[c], yj[c]);
+    d2 = __fadd_rn(d2, __fmul_rn(diff[c], diff[c]));
+  }
+  d2 = fmaxf(d2, 1e-6f);
+  const float pw = powf(d2, p.b);
+  const float num = __fmul_rn(__fmul_rn(__fmul_rn(-2.0f, p.a), p.b), powf(d2, p.bm1));
+  const float coeff = __fdiv_rn(num, __fadd_rn(1.0f, __fmul_rn(p.a, pw)));
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) out[c] = __fmul_rn(fminf(fmaxf(__fmul_rn(coeff, diff[c]), -4.0f), 4.0f), p.alpha);
+}
+
+template <int DIM>
+__device__ __forceinline__ void repel_add(const float (&yi)[DIM], const float (&yt)[DIM], const Params& p,
+                                          float (&acc)[DIM]) {
+  float diff[DIM];
+  float d2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    diff[c] = __fsub_rn(yi[c], yt[c]);
+    d2 = __fadd_rn(d2, __fmul_rn(diff[c], diff[c]));
+  }
+  d2 = fmaxf(d2, 1e-6f);
+  const float pw = powf(d2, p.b);
+  const float den = __fmul_rn(__fadd_rn(0.001f, d2), __fadd_rn(1.0f, __fmul_rn(p.a, pw)));
+  const float coeff = __fdiv_rn(p.two_b, den);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c)
+    acc[c] = __fadd_rn(acc[c], __fmul_rn(fminf(fmaxf(__fmul_rn(coeff, diff[c]), -4.0f), 4.0f), p.alpha));
+}
+
+template <int DIM>
+__device__ __forceinline__ void load_row(const float* __restrict__ Y, int i, float (&v)[DIM]) {
+  if constexpr (DIM == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2*>(Y) + i);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else if constexpr (DIM == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(Y) + i);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  } else {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) v[c] = __ldg(Y + (int64_t)i * DIM + c);
+  }
+}
+
+template <int DIM>
+__device__ __forceinline__ void atomic_add_row(float* __restrict__ dY, int i, const float (&v)[DIM]) {
+  if constexpr (DIM == 2) {
+    atomicAdd(reinterpret_cast<float2*>(dY) + i, make_float2(v[0], v[1]));
+  } else if constexpr (DIM == 4) {
+    atomicAdd(reinterpret_cast<float4*>(dY) + i, make_float4(v[0], v[1], v[2], v[3]));
+  } else {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) atomicAdd(dY + (int64_t)i * DIM + c, v[c]);
+  }
+}
+
+// ---- schedule ----------------------------------------------------------------
+__global__ void max_kernel(const float* __restrict__ vals, const int64_t* __restrict__ n_edges, float* __restrict__ wmax) {
+  const int64_t E = *n_edges;
+  float m = 0.f;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, vals[e]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(wmax), __float_as_int(m));
+}
+
+__global__ void eps_kernel(const float* __restrict__ vals, const int64_t* __restrict__ n_edges,
+                           const float* __restrict__ wmax, int n_epochs, float* __restrict__ eps,
+                           float* __restrict__ next) {
+  const int64_t E = *n_edges;
+  const float wm = *wmax;
+  const float ne = (float)n_epochs;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    const float ns = __fmul_rn(ne, __fdiv_rn(vals[e], wm));
+    const float v = ns > 0.f ? __fdiv_rn(ne, ns) : -1.0f;
+    eps[e] = v;
+    next[e] = v;
+  }
+}
+
+// ---- fast path epoch ---------------------------------------------------------
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY, int n,
+                                                           const int32_t* __restrict__ rows,
+                                                           const int32_t* __restrict__ cols,
+                                                           const float* __restrict__ eps, float* __restrict__ next,
+                                                           const int64_t* __restrict__ n_edges, int epoch, Params p,
+                                                           int neg_rate, uint32_t k0, uint32_t k1) {
+  const int64_t E = *n_edges;
+  const float ep = (float)epoch;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    const float nx = next[e];
+    if (!(nx <= ep)) continue;
+    next[e] = __fadd_rn(nx, eps[e]);
+    const int i = rows[e], j = cols[e];
+    float yi[DIM], yj[DIM], acc[DIM], pos[DIM];
+    load_row<DIM>(Y, i, yi);
+    load_row<DIM>(Y, j, yj);
+    attract<DIM>(yi, yj, p, pos);
+    float neg_pos[DIM];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      acc[c] = pos[c];
+      neg_pos[c] = -pos[c];
+    }
+    atomic_add_row<DIM>(dY, j, neg_pos);
+    for (int m0 = 0; m0 < neg_rate; m0 += 4) {
+      const U4 r = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, (uint32_t)(m0 >> 2)}, k0, k1);
+      const uint32_t rs[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (m0 + u < neg_rate) {
+          float yt[DIM];
+          load_row<DIM>(Y, to_range(rs[u], (uint32_t)n), yt);
+          repel_add<DIM>(yi, yt, p, acc);
+        }
+      }
+    }
+    atomic_add_row<DIM>(dY, i, acc);
+  }
+}
+
+__global__ void apply_kernel(float* __restrict__ Y, float* __restrict__ dY, int64_t m) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    Y[t] = __fadd_rn(Y[t], dY[t]);
+    dY[t] = 0.f;
+  }
+}
+
+// ---- injected path (reference-ordered negatives) ------------------------------
+__global__ void count_active_kernel(const float* __restrict__ next, const int64_t* __restrict__ n_edges, int epoch,
+                                    int32_t* __restrict__ block_counts) {
+  __shared__ int warp_counts[kBlock / 32];
+  const int64_t E = *n_edges;
+  const float ep = (float)epoch;
+  const int64_t base = (int64_t)blockIdx.x * kEdgesPerBlock;
+  int c = 0;
+  for (int u = 0; u < kEdgesPerBlock / kBlock; ++u) {
+    const int64_t e = base + u * kBlock + threadIdx.x;
+    c += (e < E && next[e] <= ep) ? 1 : 0;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) warp_counts[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int i = 0; i < kBlock / 32; ++i) t += warp_counts[i];
+    block_counts[blockIdx.x] = t;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kBlock) sgd_injected_kernel(
+    const float* __restrict__ Y, float* __restrict__ dY, const int32_t* __restrict__ rows,
+    const int32_t* __restrict__ cols, const float* __restrict__ eps, float* __restrict__ next,
+    const int64_t* __restrict__ n_edges, int epoch, Params p, int neg_rate, const int32_t* __restrict__ neg_to,
+    const int32_t* __restrict__ block_offsets, const int64_t* __restrict__ n_active) {
+  __shared__ int warp_base[kBlock / 32];
+  __shared__ int running;
+  const int64_t E = *n_edges;
+  const int64_t A = *n_active;
+  const float ep = (float)epoch;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) running = block_offsets[blockIdx.x];
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kEdgesPerBlock;
+  for (int u = 0; u < kEdgesPerBlock / kBlock; ++u) {
+    const int64_t e = base + u * kBlock + threadIdx.x;
+    const float nx = e < E ? next[e] : 1.0f;
+    const bool act = e < E && nx <= ep;
+    const unsigned ballot = __ballot_sync(0xffffffffu, act);
+    if (lane == 0) warp_base[warp] = __popc(ballot);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = running;
+      for (int w = 0; w < kBlock / 32; ++w) {
+        const int c = warp_base[w];
+        warp_base[w] = s;
+        s += c;
+      }
+      running = s;
+    }
+    __syncthreads();
+    if (act) {
+      const int64_t rank = warp_base[warp] + __popc(ballot & ((1u << lane) - 1u));
+      next[e] = __fadd_rn(nx, eps[e]);
+      const int i = rows[e], j = cols[e];
+      float yi[DIM], yj[DIM], acc[DIM], pos[DIM], neg_pos[DIM];
+      load_row<DIM>(Y, i, yi);
+      load_row<DIM>(Y, j, yj);
+      attract<DIM>(yi, yj, p, pos);
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        acc[c] = pos[c];
+        neg_pos[c] = -pos[c];
+      }
+      atomic_add_row<DIM>(dY, j, neg_pos);
+      for (int m = 0; m < neg_rate; ++m) {
+        float yt[DIM];
+        load_row<DIM>(Y, neg_to[rank + (int64_t)m * A], yt);
+        repel_add<DIM>(yi, yt, p, acc);
+      }
+      atomic_add_row<DIM>(dY, i, acc);
+    }
+    __syncthreads();
+  }
+}
+
+struct Layout {
+  int32_t* status;
+  float* dY;
+  float* wmax;
+  int32_t* block_counts;
+  int64_t* total;
+  size_t bytes;
+};
+
+static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap) {
+  Carver c(ws);
+  Layout l;
+  l.status = c.take<int32_t>(64);
+  l.wmax = c.take<float>(64);
+  l.dY = c.take<float>((size_t)n * dim);
+  l.block_counts = c.take<int32_t>((size_t)ceil_div(e_cap > 0 ? e_cap : 1, kEdgesPerBlock) + 1);
+  l.total = c.take<int64_t>(8);
+  l.bytes = c.bytes();
+  return l;
+}
+
+static Params make_params(float a, float b, float lr, int epoch, int n_epochs) {
+  Params p;
+  p.a = a;
+  p.b = b;
+  p.bm1 = b - 1.0f;
+  p.two_b = 2.0f * b;
+  // the reference computes alpha in Python double and casts it to float32 (umap.py:431)
+  p.alpha = (float)((double)lr * (1.0 - (double)epoch / (double)n_epochs));
+  return p;
+}
+
+static unsigned edge_grid(int64_t e_cap) {
+  const int64_t want = ceil_div(e_cap > 0 ? e_cap : 1, kBlock);
+  const int64_t cap = (int64_t)num_sms() * 16;
+  return (unsigned)(want < cap ? want : cap);
+}
+
+template <int DIM>
+static void launch_epoch(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
+                         const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
+                         const Params& p, int neg_rate, uint64_t seed, cudaStream_t stream) {
+  sgd_epoch_kernel<DIM><<<edge_grid(e_cap), kBlock, 0, stream>>>(Y, l.dY, (int)n, rows, cols, eps, next, n_edges,
+                                                                 epoch, p, neg_rate, (uint32_t)seed,
+                                                                 (uint32_t)(seed >> 32));
+  const int64_t m = n * DIM;
+  const unsigned gb = (unsigned)(ceil_div(m, kBlock) < num_sms() * 8 ? ceil_div(m, kBlock) : num_sms() * 8);
+  apply_kernel<<<gb, kBlock, 0, stream>>>(Y, l.dY, m);
+}
+
+template <int DIM>
+static void launch_injected(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
+                            const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
+                            const Params& p, int neg_rate, const int32_t* neg_to, cudaStream_t stream) {
+  const unsigned nb = (unsigned)ceil_div(e_cap > 0 ? e_cap : 1, kEdgesPerBlock);
+  sgd_injected_kernel<DIM><<<nb, kBlock, 0, stream>>>(Y, l.dY, rows, cols, eps, next, n_edges, epoch, p, neg_rate,
+                                                      neg_to, l.block_counts, l.total);
+  const int64_t m = n * DIM;
+  apply_kernel<<<(unsigned)ceil_div(m, kBlock), kBlock, 0, stream>>>(Y, l.dY, m);
+}
+
+}  // namespace layout
+}  // namespace umapb
+
+using namespace umapb;
+
+extern "C" int umapb_layout_workspace(int64_t n, int32_t dim, int64_t e_cap, size_t* bytes) {
+  clear_error();
+  UMAPB_REQUIRE(bytes, "bytes is null");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4 && e_cap >= 0, "layout: need n >= 1, 1 <= dim <= 4, e_cap >= 0");
+  *bytes = layout::carve(nullptr, n, dim, e_cap).bytes;
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_layout_prepare(const float* vals, const int64_t* n_edges, int64_t e_cap, int32_t n_epochs,
+                                    float* eps, float* next, void* workspace, size_t workspace_bytes,
+                                    umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(vals && n_edges && eps && next, "layout_prepare: null array argument");
+  UMAPB_REQUIRE(n_epochs >= 1, "layout_prepare: n_epochs must be >= 1");
+  UMAPB_REQUIRE(workspace && workspace_bytes >= 512, "layout_prepare: workspace too small");
+  layout::Layout l = layout::carve(workspace, 1, 1, 1);  // status and wmax sit at fixed offsets
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.wmax, 0, 4, stream), "layout_prepare: reset");
+  const unsigned g = layout::edge_grid(e_cap);
+  layout::max_kernel<<<g, layout::kBlock, 0, stream>>>(vals, n_edges, l.wmax);
+  layout::eps_kernel<<<g, layout::kBlock, 0, stream>>>(vals, n_edges, l.wmax, n_epochs, eps, next);
+  UMAPB_LAUNCH_CHECK("layout_prepare kernels");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                                   const float* eps, float* next, const int64_t* n_edges, int64_t e_cap,
+                                   int32_t epoch_begin, int32_t epoch_end, int32_t n_epochs, float a, float b,
+                                   float learning_rate, int32_t neg_rate, uint64_t seed, void* workspace,
+                                   size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(Y && rows && cols && eps && next && n_edges, "layout_epochs: null array argument");
+  UMAPB_REQUIRE(n >= 1 && n < ((int64_t)1 << 31), "layout_epochs: need 1 <= n < 2^31");
+  UMAPB_REQUIRE(dim >= 1 && dim <= 4, "layout_epochs: dim must be in [1, 4]");
+  UMAPB_REQUIRE(neg_rate >= 0, "layout_epochs: negative_sample_rate must be >= 0");
+  UMAPB_REQUIRE(0 <= epoch_begin && epoch_begin <= epoch_end && epoch_end <= n_epochs,
+                "layout_epochs: need 0 <= epoch_begin <= epoch_end <= n_epochs");
+  layout::Layout l = layout::carve(nullptr, n, dim, e_cap);
+  if (!workspace || workspace_bytes < l.bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "layout: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
+  l = layout::carve(workspace, n, dim, e_cap);
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epochs: reset");
+  for (int ep = epoch_begin; ep < epoch_end; ++ep) {
+    const layout::Params p = layout::make_params(a, b, learning_rate, ep, n_epochs);
+    switch (dim) {
+      case 1: layout::launch_epoch<1>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
+      case 2: layout::launch_epoch<2>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
+      case 3: layout::launch_epoch<3>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
+      default: layout::launch_epoch<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
+    }
+  }
+  UMAPB_LAUNCH_CHECK("layout_epochs kernels");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_layout_count_active(const float* next, const int64_t* n_edges, int64_t n, int32_t dim,
+                                         int64_t e_cap, int32_t epoch, int64_t* count, void* workspace,
+                                         size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(next && n_edges && count, "layout_count_active: null array argument");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4, "layout_count_active: need n >= 1 and 1 <= dim <= 4");
+  layout::Layout l = layout::carve(nullptr, n, dim, e_cap);
+  if (!workspace || workspace_bytes < l.bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "layout: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
+  l = layout::carve(workspace, n, dim, e_cap);
+  const int64_t nb = ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
+  layout::count_active_kernel<<<(unsigned)nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
+  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, nb, count);
+  UMAPB_LAUNCH_CHECK("layout_count_active kernels");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, const int32_t* rows,
+                                           const int32_t* cols, const float* eps, float* next,
+                                           const int64_t* n_edges, int64_t e_cap, int32_t epoch, int32_t n_epochs,
+                                           float a, float b, float learning_rate, int32_t neg_rate,
+                                           const int32_t* neg_to, int64_t neg_count, void* workspace,
+                                           size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(Y && rows && cols && eps && next && n_edges, "layout_epoch_injected: null array argument");
+  UMAPB_REQUIRE(dim >= 1 && dim <= 4, "layout_epoch_injected: dim must be in [1, 4]");
+  UMAPB_REQUIRE(0 <= epoch && epoch < n_epochs, "layout_epoch_injected: epoch out of range");
+  UMAPB_REQUIRE(neg_rate >= 0 && neg_count >= 0, "layout_epoch_injected: negative counts must be >= 0");
+  UMAPB_REQUIRE(neg_to || neg_count == 0, "layout_epoch_injected: neg_to is null");
+  layout::Layout l = layout::carve(nullptr, n, dim, e_cap);
+  if (!workspace || workspace_bytes < l.bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "layout: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
+  l = layout::carve(workspace, n, dim, e_cap);
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epoch_injected: reset");
+  const unsigned nb = (unsigned)ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
+  layout::count_active_kernel<<<nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
+  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, (int64_t)nb, l.total);
+  UMAPB_LAUNCH_CHECK("layout_epoch_injected: active count");
+  int64_t active = 0;
+  UMAPB_CUDA_TRY(cudaMemcpyAsync(&active, l.total, sizeof(active), cudaMemcpyDeviceToHost, stream),
+                 "layout_epoch_injected: count readback");
+  UMAPB_CUDA_TRY(cudaStreamSynchronize(stream), "layout_epoch_injected: sync");
+  if (active * neg_rate != neg_count)
+    return set_error(UMAPB_ERR_ARG, "layout_epoch_injected: epoch %d has %lld active edges, so %lld negatives are "
+                     "needed (got %lld)", epoch, (long long)active, (long long)(active * neg_rate),
+                     (long long)neg_count);
+  const layout::Params p = layout::make_params(a, b, learning_rate, epoch, n_epochs);
+  switch (dim) {
+    case 1: layout::launch_injected<1>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch, p, neg_rate, neg_to, stream); break;
+    case 2: layout::launch_injected<2>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch, p, neg_rate, neg_to, stream); break;
+    case 3: layout::launch_injected<3>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch, p, neg_rate, neg_to, stream); break;
+    default: layout::launch_injected<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch, p, neg_rate, neg_to, stream); break;
+  }
+  UMAPB_LAUNCH_CHECK("layout_epoch_injected kernels");
+  return UMAPB_OK;
+}

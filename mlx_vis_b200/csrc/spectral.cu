@@ -1,0 +1,324 @@
+// Spectral initialisation — replaces UMAP._spectral_init, mlx_vis/_umap/umap.py:298-348.
+//
+// The reference: degrees by scatter-add (float32, edge order), d^-1/2, normalised
+// weights w * d_r^-1/2 * d_c^-1/2, then 100 x { V = W V (gather + scatter-add);
+// modified Gram-Schmidt with norm sqrt(|v|^2 + 1e-10) } on V (n x (c+1)), take
+// columns 1..c, scale by 10 / max|e|, add N(0, 1e-4) noise (NumPy, host) and
+// min-max each column to [0, 10].
+//
+// Here the edges are in row-major order, so W V is a CSR SpMV without atomics
+// (one thread per row, edges summed in the reference's order).  MGS of the
+// (c+1)-column block equals Q = V R^-1 with R the Cholesky factor of the Gram
+// matrix V^T V (+1e-10 on each pivot, as in the reference's norms), so each
+// iteration is ONE kernel: it applies the previous iteration's R^-1 to every
+// gathered row on the fly and accumulates the new Gram matrix in FP64.
+#include <math.h>
+
+#include "common.cuh"
+#include "philox.cuh"
+
+namespace umapb {
+namespace spectral {
+
+constexpr int kBlock = 256;
+constexpr int kMaxCols = 5;  // n_components <= 4
+
+__global__ void row_ptr_kernel(const int32_t* __restrict__ rows, const int64_t* __restrict__ n_edges, int64_t n,
+                               int64_t* __restrict__ row_ptr) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r > n) return;
+  const int64_t E = *n_edges;
+  int64_t lo = 0, hi = E;  // lower_bound of r in rows[0, E)
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (rows[mid] < r) lo = mid + 1;
+    else hi = mid;
+  }
+  row_ptr[r] = lo;
+}
+
+// degree (float32, reference edge order), then normalised weights
+__global__ void degree_kernel(const float* __restrict__ vals, const int64_t* __restrict__ row_ptr, int64_t n,
+                              float* __restrict__ dis) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  float d = 0.f;
+  for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e) d = __fadd_rn(d, vals[e]);
+  d = fmaxf(d, 1e-10f);
+  dis[r] = __fdiv_rn(1.0f, sqrtf(d));
+}
+
+__global__ void norm_weight_kernel(const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+                                   const float* __restrict__ vals, const int64_t* __restrict__ n_edges,
+                                   const float* __restrict__ dis, float* __restrict__ wn) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= *n_edges) return;
+  wn[e] = __fmul_rn(__fmul_rn(vals[e], dis[rows[e]]), dis[cols[e]]);
+}
+
+// R (upper triangular) from the Gram matrix G with pivots sqrt(g - sum r^2 + 1e-10);
+// returns Rinv (upper triangular) in `ri`.  kk <= kMaxCols.
+__device__ void chol_inverse(const double* G, int kk, double* ri) {
+  double R[kMaxCols][kMaxCols];
+  for (int j = 0; j < kk; ++j) {
+    for (int i = 0; i < j; ++i) {
+      double s = G[i * kk + j];
+      for (int p = 0; p < i; ++p) s -= R[p][i] * R[p][j];
+      R[i][j] = s / R[i][i];
+    }
+    double s = G[j * kk + j];
+    for (int p = 0; p < j; ++p) s -= R[p][j] * R[p][j];
+    R[j][j] = sqrt(fmax(s, 0.0) + 1e-10);
+    for (int i = j + 1; i < kk; ++i) R[i][j] = 0.0;
+  }
+  // invert the upper-triangular R column by column
+  for (int j = 0; j < kk; ++j) {
+    for (int i = kk - 1; i >= 0; --i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int p = i + 1; p < kk; ++p) s -= R[i][p] * ri[p * kk + j];
+      ri[i * kk + j] = (i <= j) ? s / R[i][i] : 0.0;
+    }
+  }
+}
+
+// One power iteration: Vout = W (Vin Rinv_prev); G_out += Vout^T Vout.
+// G_prev == nullptr means Rinv = I (the first multiplication uses V0 as is).
+__global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* __restrict__ G_prev,
+                                 const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
+                                 const float* __restrict__ wn, int64_t n, int kk, double* __restrict__ Vout,
+                                 double* __restrict__ G_out) {
+  __shared__ double ri[kMaxCols * kMaxCols];
+  __shared__ double gsum[kBlock / 32][kMaxCols * kMaxCols];
+  if (threadIdx.x == 0) {
+    if (G_prev) {
+      chol_inverse(G_prev, kk, ri);
+    } else {
+      for (int i = 0; i < kk * kk; ++i) ri[i] = (i % (kk + 1) == 0) ? 1.0 : 0.0;
+    }
+  }
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[kMaxCols] = {0, 0, 0, 0, 0};
+  if (r < n) {
+    for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e) {
+      const int64_t c = cols[e];
+      const double w = (double)wn[e];
+      double v[kMaxCols];
+      for (int j = 0; j < kk; ++j) v[j] = Vin[c * kk + j];
+      for (int j = 0; j < kk; ++j) {  // q_j = sum_i v_i Rinv[i][j]
+        double q = 0.0;
+        for (int i = 0; i <= j; ++i) q += v[i] * ri[i * kk + j];
+        acc[j] += w * q;
+      }
+    }
+    for (int j = 0; j < kk; ++j) Vout[r * kk + j] = acc[j];
+  }
+  // block reduction of the Gram matrix
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = 0; i < kk; ++i) {
+    for (int j = i; j < kk; ++j) {
+      double g = acc[i] * acc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+      if (lane == 0) gsum[warp][i * kk + j] = g;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kk * kk) {
+    const int i = threadIdx.x / kk, j = threadIdx.x % kk;
+    if (i <= j) {
+      double g = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) g += gsum[w][i * kk + j];
+      atomicAdd(&G_out[i * kk + j], g);
+      if (i != j) atomicAdd(&G_out[j * kk + i], g);
+    }
+  }
+}
+
+__device__ __forceinline__ unsigned f2ord(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// embedding = (V R^-1)[:, 1:], max |embedding|
+__global__ void finish_orth_kernel(const double* __restrict__ V, const double* __restrict__ G, int64_t n, int kk,
+                                   float* __restrict__ emb, unsigned* __restrict__ absmax) {
+  __shared__ double ri[kMaxCols * kMaxCols];
+  if (threadIdx.x == 0) chol_inverse(G, kk, ri);
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float m = 0.f;
+  if (r < n) {
+    for (int j = 1; j < kk; ++j) {
+      double q = 0.0;
+      for (int i = 0; i <= j; ++i) q += V[r * kk + i] * ri[i * kk + j];
+      const float f = (float)q;
+      emb[r * (kk - 1) + (j - 1)] = f;
+      m = fmaxf(m, fabsf(f));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(absmax, __float_as_uint(m));
+}
+
+// e = f32(emb * (10 / max|emb|)) + noise (umap.py:344-346); per-column min/max
+__global__ void scale_noise_kernel(float* __restrict__ emb, const float* __restrict__ noise, int64_t n, int dim,
+                                   const unsigned* __restrict__ absmax, unsigned* __restrict__ colmin,
+                                   unsigned* __restrict__ colmax) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const float expansion = __fdiv_rn(10.0f, __uint_as_float(*absmax));
+  if (t < n * dim) {
+    const float v = __fadd_rn(__fmul_rn(emb[t], expansion), noise[t]);
+    emb[t] = v;
+    const int c = (int)(t % dim);
+    atomicMin(&colmin[c], f2ord(v));
+    atomicMax(&colmax[c], f2ord(v));
+  }
+}
+
+// Y = 10 (e - min) / (max - min + 1e-10) per column (umap.py:347)
+__global__ void minmax_kernel(const float* __restrict__ emb, int64_t n, int dim, const unsigned* __restrict__ colmin,
+                              const unsigned* __restrict__ colmax, float* __restrict__ Y) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * dim) return;
+  const int c = (int)(t % dim);
+  const float mn = ord2f(colmin[c]), mx = ord2f(colmax[c]);
+  const float num = __fmul_rn(10.0f, __fsub_rn(emb[t], mn));
+  const float den = __fadd_rn(__fsub_rn(mx, mn), 1e-10f);
+  Y[t] = __fdiv_rn(num, den);
+}
+
+struct Layout {
+  int32_t* status;
+  int64_t* row_ptr;
+  float* dis;
+  float* wn;
+  double* V[2];
+  double* G;  // n_iter blocks of kk*kk
+  float* emb;
+  unsigned* red;  // absmax, colmin[4], colmax[4]
+  size_t bytes;
+};
+
+static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
+  const int kk = dim + 1;
+  Carver c(ws);
+  Layout l;
+  l.status = c.take<int32_t>(64);
+  l.row_ptr = c.take<int64_t>((size_t)n + 1);
+  l.dis = c.take<float>((size_t)n);
+  l.wn = c.take<float>((size_t)(e_cap > 0 ? e_cap : 1));
+  l.V[0] = c.take<double>((size_t)n * kk);
+  l.V[1] = c.take<double>((size_t)n * kk);
+  l.G = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
+  l.emb = c.take<float>((size_t)n * dim);
+  l.red = c.take<unsigned>(16);
+  l.bytes = c.bytes();
+  return l;
+}
+
+__global__ void f32_to_f64_kernel(const float* __restrict__ a, double* __restrict__ b, int64_t m) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < m) b[t] = (double)a[t];
+}
+
+// Standard normal draws: element i of the stream (seed) comes from Philox block i/4
+// and the Box-Muller transform of its two 32-bit pairs.
+__global__ void normal_fill_kernel(float* __restrict__ out, int64_t count, uint32_t k0, uint32_t k1) {
+  const int64_t blk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk * 4 >= count) return;
+  const U4 r = philox4x32_10(U4{(uint32_t)blk, (uint32_t)(blk >> 32), 0x5eedu, 0u}, k0, k1);
+  float s0, c0, s1, c1;
+  const float r0 = sqrtf(-2.0f * logf(to_unit(r.x)));
+  const float r1 = sqrtf(-2.0f * logf(to_unit(r.z)));
+  sincospif(2.0f * to_unit(r.y), &s0, &c0);
+  sincospif(2.0f * to_unit(r.w), &s1, &c1);
+  const float z[4] = {r0 * c0, r0 * s0, r1 * c1, r1 * s1};
+  for (int u = 0; u < 4; ++u)
+    if (blk * 4 + u < count) out[blk * 4 + u] = z[u];
+}
+
+__global__ void init_red_kernel(unsigned* red, int dim) {
+  if (threadIdx.x == 0) red[0] = 0u;
+  if (threadIdx.x < (unsigned)dim) {
+    red[1 + threadIdx.x] = 0xFFFFFFFFu;  // min
+    red[5 + threadIdx.x] = 0u;           // max
+  }
+}
+
+}  // namespace spectral
+}  // namespace umapb
+
+using namespace umapb;
+
+extern "C" int umapb_spectral_workspace(int64_t n, int32_t dim, int64_t e_cap, int32_t n_iter, size_t* bytes) {
+  clear_error();
+  UMAPB_REQUIRE(bytes, "bytes is null");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4, "spectral: need n >= 1 and 1 <= dim <= 4");
+  UMAPB_REQUIRE(n_iter >= 1 && n_iter <= 128, "spectral: need 1 <= n_iter <= 128");
+  UMAPB_REQUIRE(e_cap >= 0, "spectral: e_cap must be >= 0");
+  *bytes = spectral::carve(nullptr, n, dim, e_cap, n_iter).bytes;
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const float* vals, const int64_t* n_edges,
+                              int64_t e_cap, int64_t n, int32_t dim, const float* V0, int32_t n_iter,
+                              const float* noise, float* Y, void* workspace, size_t workspace_bytes,
+                              umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(rows && cols && vals && n_edges && V0 && noise && Y, "spectral: null array argument");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4, "spectral: need n >= 1 and 1 <= dim <= 4");
+  UMAPB_REQUIRE(n_iter >= 1 && n_iter <= 128, "spectral: need 1 <= n_iter <= 128");
+  UMAPB_REQUIRE(e_cap >= 0, "spectral: e_cap must be >= 0");
+  spectral::Layout l = spectral::carve(nullptr, n, dim, e_cap, n_iter);
+  if (!workspace || workspace_bytes < l.bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "spectral: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
+  l = spectral::carve(workspace, n, dim, e_cap, n_iter);
+  const int kk = dim + 1;
+  const unsigned rb = (unsigned)ceil_div(n, spectral::kBlock);
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.status, 0, 4, stream), "spectral: status reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.G, 0, sizeof(double) * n_iter * kk * kk, stream), "spectral: gram reset");
+  spectral::row_ptr_kernel<<<(unsigned)ceil_div(n + 1, spectral::kBlock), spectral::kBlock, 0, stream>>>(
+      rows, n_edges, n, l.row_ptr);
+  spectral::degree_kernel<<<rb, spectral::kBlock, 0, stream>>>(vals, l.row_ptr, n, l.dis);
+  if (e_cap > 0)
+    spectral::norm_weight_kernel<<<(unsigned)ceil_div(e_cap, spectral::kBlock), spectral::kBlock, 0, stream>>>(
+        rows, cols, vals, n_edges, l.dis, l.wn);
+  spectral::f32_to_f64_kernel<<<(unsigned)ceil_div(n * kk, spectral::kBlock), spectral::kBlock, 0, stream>>>(
+      V0, l.V[0], n * kk);
+  UMAPB_LAUNCH_CHECK("spectral: setup kernels");
+  for (int it = 0; it < n_iter; ++it) {
+    const double* gprev = it == 0 ? nullptr : l.G + (size_t)(it - 1) * kk * kk;
+    spectral::spmv_gram_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[it & 1], gprev, l.row_ptr, cols, l.wn, n,
+                                                                     kk, l.V[(it + 1) & 1],
+                                                                     l.G + (size_t)it * kk * kk);
+  }
+  UMAPB_LAUNCH_CHECK("spectral: power iteration");
+  spectral::init_red_kernel<<<1, 32, 0, stream>>>(l.red, dim);
+  spectral::finish_orth_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[n_iter & 1],
+                                                                     l.G + (size_t)(n_iter - 1) * kk * kk, n, kk,
+                                                                     l.emb, l.red);
+  const unsigned eb = (unsigned)ceil_div(n * dim, spectral::kBlock);
+  spectral::scale_noise_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, noise, n, dim, l.red, l.red + 1,
+                                                                     l.red + 5);
+  spectral::minmax_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, n, dim, l.red + 1, l.red + 5, Y);
+  UMAPB_LAUNCH_CHECK("spectral: rescale kernels");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_normal_fill(float* out, int64_t count, uint64_t seed, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(out || count == 0, "normal_fill: null output");
+  UMAPB_REQUIRE(count >= 0, "normal_fill: count must be >= 0");
+  if (count == 0) return UMAPB_OK;
+  const int64_t blocks4 = ceil_div(count, 4);
+  spectral::normal_fill_kernel<<<(unsigned)ceil_div(blocks4, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
+      out, count, (uint32_t)seed, (uint32_t)(seed >> 32));
+  UMAPB_LAUNCH_CHECK("normal_fill kernel");
+  return UMAPB_OK;
+}

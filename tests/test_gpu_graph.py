@@ -1,0 +1,130 @@
+"""Fuzzy simplicial set, spectral initialisation and layout epochs on the GPU
+against the reference's golden vectors and the CPU oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fuzzy as ofz
+from oracle import layout as olay
+from oracle import spectral as ospec
+
+pytestmark = pytest.mark.gpu
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def gpu_fuzzy(idx, dist, n_epochs, fp64):
+    from mlx_vis_b200 import _lib
+
+    r, c, v, ne, rho, sig = _lib.fuzzy(cuda(idx.astype(np.int32)), cuda(dist.astype(np.float32)), n_epochs,
+                                       fp64=fp64, with_sigma=True)
+    E = int(ne.item())
+    return (r[:E].cpu().numpy(), c[:E].cpu().numpy(), v[:E].cpu().numpy()), (rho.cpu().numpy(), sig.cpu().numpy())
+
+
+@pytest.mark.parametrize("name,n_epochs", [("fuzzy_gauss", 200), ("fuzzy_dups", 500)])
+def test_fuzzy_fp64_matches_fp64_oracle(name, n_epochs, golden):
+    g = golden(name)
+    if name == "fuzzy_gauss":
+        kb = golden("knn_brute_gauss")
+        idx, dist = kb["idx"], kb["dist"]
+    else:
+        idx, dist = g["knn_idx"], g["knn_dist"]
+    (r, c, v), (rho, sig) = gpu_fuzzy(idx, dist, n_epochs, fp64=True)
+    (ro, co, vo), (rho_o, sig_o) = ofz.fuzzy_simplicial_set(idx, dist, n_epochs, dtype=np.float64)
+    assert np.array_equal(r, ro) and np.array_equal(c, co)
+    np.testing.assert_allclose(v, vo, rtol=1e-6)
+    np.testing.assert_allclose(sig, sig_o.astype(np.float32), rtol=1e-6)
+    # and against the reference (float32 bisection): same edge set, weights within its tolerance band
+    assert np.array_equal(r, g["rows"]) and np.array_equal(c, g["cols"])
+    rel = np.abs(v - g["vals"]) / g["vals"]
+    assert rel.max() < 5e-5 and np.mean(rel < 1e-5) > 0.99
+
+
+@pytest.mark.parametrize("name,n_epochs", [("fuzzy_gauss", 200), ("fuzzy_dups", 500)])
+def test_fuzzy_fp32_mode_matches_reference(name, n_epochs, golden):
+    g = golden(name)
+    if name == "fuzzy_gauss":
+        kb = golden("knn_brute_gauss")
+        idx, dist = kb["idx"], kb["dist"]
+    else:
+        idx, dist = g["knn_idx"], g["knn_dist"]
+    (r, c, v), _ = gpu_fuzzy(idx, dist, n_epochs, fp64=False)
+    assert np.array_equal(r, g["rows"]) and np.array_equal(c, g["cols"])
+    rel = np.abs(v - g["vals"]) / g["vals"]
+    assert np.mean(rel <= 1e-5) > 0.999 and rel.max() < 5e-5
+
+
+def test_spectral_matches_reference_with_injected_draws(golden):
+    from mlx_vis_b200 import _lib
+
+    fz, sp = golden("fuzzy_gauss"), golden("spectral_gauss")
+    n = 2000
+    rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
+    ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
+    noise = np.random.RandomState(42).normal(scale=0.0001, size=(n, 2)).astype(np.float32)
+    Y = _lib.spectral(rows, cols, vals, ne, n, 2, cuda(sp["V0"]), cuda(noise), n_iter=100).cpu().numpy()
+    Y64 = ospec.spectral_init(fz["rows"], fz["cols"], fz["vals"], n, sp["V0"], 0, dtype=np.float64)
+    assert np.abs(Y - Y64).max() < 1e-4
+    assert np.abs(Y - sp["Y0"]).max() < 1e-3
+
+
+def _layout(fz, n=2000, n_epochs=200):
+    from mlx_vis_b200 import _lib
+
+    rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
+    ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
+    return _lib.Layout(rows, cols, vals, ne, n, 2, n_epochs)
+
+
+def test_schedule_active_counts_match_reference(golden, manifest):
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    lay = _layout(fz)
+    Y = cuda(opt["Y_ep0"].copy())
+    counts = []
+    for e in range(200):
+        counts.append(lay.count_active(e))
+        lay.epochs(Y, e, e + 1, m["a"], m["b"], 1.0, 5, 1234)
+    assert counts == list(opt["n_active"])
+
+
+def test_injected_epochs_match_reference(golden, manifest):
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    lay = _layout(fz)
+    Y = cuda(opt["Y_ep0"].copy())
+    nonempty = [e for e in range(200) if opt["n_active"][e] > 0]
+    scale = float(np.abs(opt["Y_ep0"]).max())
+    for j, e in enumerate(nonempty[:3]):
+        # epochs before the first non-empty one do nothing
+        lay.epochs(Y, (nonempty[j - 1] + 1) if j else 0, e, m["a"], m["b"], 1.0, 5, 0)
+        lay.epoch_injected(Y, e, m["a"], m["b"], 1.0, 5, cuda(opt[f"neg_{j}"].astype(np.int32)))
+        if j == 0:
+            got = Y.cpu().numpy()
+            ref = opt[f"Y_ep{e + 1}"]
+            # one epoch: within 1e-5 of the reference coordinates (relative to their scale)
+            assert np.abs(got - ref).max() <= 1e-5 * max(1.0, scale), np.abs(got - ref).max()
+            sets = olay.active_sets(fz["vals"], 200)
+            Yo = olay.sgd_epoch(opt["Y_ep0"], fz["rows"][sets[e]], fz["cols"][sets[e]],
+                                np.resize(fz["rows"][sets[e]], 5 * len(sets[e])), opt["neg_0"].astype(np.int64),
+                                1.0 * (1 - e / 200), m["a"], m["b"])
+            assert np.abs(got - Yo).max() <= 1e-5 * max(1.0, scale)
+    got = Y.cpu().numpy()
+    ref = opt[f"Y_ep{nonempty[2] + 1}"]
+    # after three epochs the steep short-range forces amplify rounding; stay close
+    assert np.median(np.abs(got - ref)) < 1e-4 and np.abs(got - ref).max() < 5e-2
+
+
+def test_injected_negative_count_is_checked(golden, manifest):
+    from mlx_vis_b200 import _lib
+
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    lay = _layout(fz)
+    Y = cuda(opt["Y_ep0"].copy())
+    with pytest.raises(_lib.UmapB200Error, match="negatives are needed"):
+        lay.epoch_injected(Y, 1, m["a"], m["b"], 1.0, 5, cuda(opt["neg_0"][:-5].astype(np.int32)))

@@ -1,0 +1,63 @@
+"""End-to-end UMAP on the GPU through the public API (drop-in for mlx_vis.UMAP)."""
+
+import numpy as np
+import pytest
+from sklearn.manifold import trustworthiness
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fit_transform_trustworthiness_matches_reference(gauss2000, manifest):
+    from mlx_vis_b200 import UMAP
+
+    ref_tw = manifest["umap_gauss"]["trustworthiness15"]
+    u = UMAP(n_components=2, n_neighbors=15, min_dist=0.1, n_epochs=200, knn_method="brute", random_state=0)
+    Y = u.fit_transform(gauss2000)
+    assert Y.shape == (2000, 2) and Y.dtype == np.float32 and np.isfinite(Y).all()
+    assert u.embedding_ is Y
+    tw = trustworthiness(gauss2000, Y, n_neighbors=15)
+    assert abs(tw - ref_tw) <= 0.005, (tw, ref_tw)
+    assert set(u.timings_) >= {"knn", "fuzzy", "init", "layout"}
+
+
+def test_graph_and_eager_epoch_loops_agree(gauss2000):
+    from mlx_vis_b200 import UMAP
+
+    ys = []
+    for use_graph in (True, False):
+        u = UMAP(n_epochs=50, knn_method="brute", random_state=3, use_graph=use_graph)
+        ys.append(u.fit_transform(gauss2000))
+    # float atomics reorder sums; the two runs may differ only by rounding-level noise
+    tw = [trustworthiness(gauss2000, y, n_neighbors=15) for y in ys]
+    assert abs(tw[0] - tw[1]) < 0.003
+
+
+def test_epoch_callback_semantics(gauss2000, golden):
+    from mlx_vis_b200 import UMAP
+
+    seen = []
+    u = UMAP(n_epochs=30, knn_method="brute", random_state=0)
+    u.fit_transform(gauss2000[:500], epoch_callback=lambda e, Y: seen.append((e, Y.shape, Y.dtype)))
+    epochs = [e for e, _, _ in seen]
+    assert epochs[0] == 0 and epochs == sorted(epochs) and all(s == (500, 2) for _, s, _ in seen)
+    assert 1 not in epochs  # epoch 0 never has active edges, so the first callback after it is epoch 2
+
+
+def test_n_epochs_default_is_written_back():
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import gaussian_mixture
+
+    X = gaussian_mixture(300, 8, seed=1)
+    u = UMAP(knn_method="brute", random_state=0)
+    u.fit_transform(X)
+    assert u.n_epochs == 500
+
+
+@pytest.mark.parametrize("n_components", [1, 3])
+def test_other_output_dims(n_components):
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import gaussian_mixture
+
+    X = gaussian_mixture(600, 16, seed=2)
+    Y = UMAP(n_components=n_components, n_epochs=60, knn_method="brute", random_state=0).fit_transform(X)
+    assert Y.shape == (600, n_components) and np.isfinite(Y).all()

@@ -1,0 +1,113 @@
+"""Pins the CPU oracle (oracle/) against golden vectors produced by the reference
+(hanxiao/mlx-vis 0.7.0 run on oracle/mlx_shim; see tests/golden/make_golden.py)."""
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from oracle import fuzzy as ofz
+from oracle import knn as oknn
+from oracle import layout as olay
+from oracle import nndescent as onnd
+from oracle import spectral as ospec
+
+
+def _sha(x):
+    return hashlib.sha256(np.ascontiguousarray(x).tobytes()).hexdigest()[:16]
+
+
+def test_generators_match_fixture_inputs(manifest, gauss2000, proto1500):
+    from mlx_vis_b200.datasets import gaussian_mixture, prototype_mixture
+
+    assert _sha(gauss2000) == manifest["knn_brute_gauss"]["sha"]
+    assert _sha(proto1500) == manifest["knn_brute_proto"]["sha"]
+    assert _sha(gaussian_mixture(3000, 32, seed=2)) == manifest["nnd_gauss"]["sha"]
+    assert _sha(prototype_mixture(2000, 784, seed=3)) == manifest["nnd_proto"]["sha"]
+
+
+@pytest.mark.parametrize("name,fixture", [("knn_brute_gauss", "gauss2000"), ("knn_brute_proto", "proto1500")])
+def test_knn_expanded_f32_matches_reference(name, fixture, golden, request):
+    X = request.getfixturevalue(fixture)
+    g = golden(name)
+    idx, dist = oknn.knn_expanded_f32(X, 15)
+    assert np.array_equal(idx, g["idx"])
+    assert np.array_equal(dist, g["dist"])
+
+
+def test_knn_exact_f64_vs_reference(gauss2000, golden):
+    g = golden("knn_brute_gauss")
+    idx, d2 = oknn.knn_exact_f64(gauss2000, 15)
+    agree = np.mean([len(set(a) & set(b)) / 15 for a, b in zip(idx, g["idx"])])
+    assert agree > 0.999
+    np.testing.assert_allclose(np.sqrt(d2), g["dist"], rtol=1e-5)
+
+
+def test_fuzzy_f32_matches_reference_exactly(golden):
+    kb, fz = golden("knn_brute_gauss"), golden("fuzzy_gauss")
+    (r, c, v), _ = ofz.fuzzy_simplicial_set(kb["idx"], kb["dist"], 200, dtype=np.float32)
+    assert np.array_equal(r, fz["rows"]) and np.array_equal(c, fz["cols"])
+    assert np.array_equal(v, fz["vals"])
+
+
+def test_fuzzy_f64_close_to_reference(golden):
+    kb, fz = golden("knn_brute_gauss"), golden("fuzzy_gauss")
+    (r, c, v), _ = ofz.fuzzy_simplicial_set(kb["idx"], kb["dist"], 200, dtype=np.float64)
+    assert np.array_equal(r, fz["rows"]) and np.array_equal(c, fz["cols"])
+    # the reference bisects in float32 and stops anywhere inside its 1e-5 band on the
+    # row sum, so float64 bisection lands ~1e-5 relative away on a few rows
+    rel = np.abs(v - fz["vals"]) / fz["vals"]
+    assert rel.max() < 5e-5
+    assert np.mean(rel < 1e-5) > 0.99
+
+
+def test_fuzzy_duplicates_edge_case(golden):
+    g = golden("fuzzy_dups")
+    (r, c, v), (rho, sigma) = ofz.fuzzy_simplicial_set(g["knn_idx"], g["knn_dist"], 500, dtype=np.float32)
+    assert np.array_equal(r, g["rows"]) and np.array_equal(c, g["cols"]) and np.array_equal(v, g["vals"])
+    assert np.all(rho > 0)
+
+
+def test_spectral_f32_matches_reference(golden):
+    fz, sp = golden("fuzzy_gauss"), golden("spectral_gauss")
+    Y0 = ospec.spectral_init(fz["rows"], fz["cols"], fz["vals"], 2000, sp["V0"], 0, dtype=np.float32)
+    assert np.array_equal(Y0, sp["Y0"])
+    Y64 = ospec.spectral_init(fz["rows"], fz["cols"], fz["vals"], 2000, sp["V0"], 0, dtype=np.float64)
+    assert np.abs(Y64 - sp["Y0"]).max() < 1e-4
+
+
+def test_schedule_matches_reference(golden):
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    sets = olay.active_sets(fz["vals"], 200)
+    assert np.array_equal([len(s) for s in sets], opt["n_active"])
+    assert len(sets[0]) == 0
+
+
+def test_one_epoch_with_injected_negatives(golden, manifest):
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    sets = olay.active_sets(fz["vals"], 200)
+    first = next(e for e in range(200) if len(sets[e]))
+    Y = olay.optimize(fz["rows"], fz["cols"], fz["vals"], opt["Y_ep0"], m["a"], m["b"], 200,
+                      lambda e, nn: opt["neg_0"].astype(np.int64), epoch_range=range(first + 1))
+    assert np.abs(Y - opt[f"Y_ep{first + 1}"]).max() < 1e-5
+
+
+@pytest.mark.parametrize("name,gen", [("nnd_gauss", ("gaussian_mixture", 3000, 32, 2)),
+                                      ("nnd_proto", ("prototype_mixture", 2000, 784, 3))])
+def test_nndescent_oracle_tracks_reference(name, gen, golden):
+    from mlx_vis_b200 import datasets
+
+    X = getattr(datasets, gen[0])(gen[1], gen[2], seed=gen[3])
+    g = golden(name)
+    its = sorted(int(k[6:]) for k in g if k.startswith("idx_it"))
+    for t in its:
+        (idx, dist), log = onnd.build(X, k=15, random_state=42, n_iters=t, history=True)
+        gi = g[f"idx_it{t}"].astype(np.int32)
+        # identical except where equal distances are ordered differently
+        row_sets = np.mean([len(set(a) & set(b)) / 15 for a, b in zip(idx, gi)])
+        assert row_sets > 0.995, (t, row_sets)
+        ours = np.array([l["changed"] for l in log])
+        ref = g[f"updates_it{t}"]
+        assert len(ours) == len(ref)
+        np.testing.assert_allclose(ours, ref, rtol=0.01, atol=10)
