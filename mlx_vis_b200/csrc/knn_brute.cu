@@ -1,7 +1,12 @@
 // Exact brute-force kNN on B200 — replaces mlx_vis/_knn.py:47-88.
 //
-// 1. prep:   X (f32) -> Xb (bf16, row pitch ld = round_up(d, 8)) and
-//            sqb[j] = |bf16(x_j)|^2 (f32); sqb = +inf for padded columns.
+// 1. prep:   X (f32) -> two BF16 operands with row pitch ld = round_up(d + 3, 8):
+//            A_i = [x~_i, 1, 1, 1, 0...] and B_j = [-2 x~_j, h1, h2, h3, 0...],
+//            x~ = bf16(x) and h1 + h2 + h3 = |x~_j|^2 (float32 split into three
+//            BF16 parts, relative error ~2^-27).  A_i . B_j is then the score
+//            s_ij = |x~_j|^2 - 2 x~_i . x~_j, which orders row i's candidates by
+//            distance (|x~_i|^2 is constant along the row).  The three extra K
+//            columns live in padding the 64-wide K blocks carry anyway.
 // 2. topk:   persistent tcgen05 kernel.  The n x n score matrix is cut into
 //            128 x 256 tiles (query rows x points); CTA c owns the contiguous
 //            tile range [c*T/G, (c+1)*T/G) in (row block, column tile) order.
@@ -9,9 +14,8 @@
 //            past n and d), warp 1 issues tcgen05.mma into one of two TMEM
 //            accumulators (2 x 256 columns), warps 4-7 read the finished
 //            accumulator (one TMEM lane = one query row per thread) and keep
-//            the row's best L scores s_j = sqb_j - 2 x_i.x_j in a sorted list in
-//            shared memory.  When the CTA leaves a row block it writes the lists
-//            to cand[row][slot] (slot = which CTA of that row block).
+//            the row's best L scores.  When the CTA leaves a row block it writes
+//            the lists to cand[row][slot] (slot = which CTA of that row block).
 // 3. rerank: one warp per row merges its slots, keeps the best L by
 //            (score, index), recomputes those L distances exactly in FP32
 //            (sum of (x_i - x_j)^2) and writes the k nearest by (distance, index).
@@ -35,10 +39,20 @@ constexpr int B_BYTES = BN * BK * 2;
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int THREADS = 256;  // warp 0 TMA, warp 1 MMA, warp 2 TMEM owner, warps 4-7 epilogue
 
+constexpr int BUF = 48;        // per-row hit buffer (entries) of the batched selection
+constexpr int MERGE_AT = 16;   // merge once some row of the warp holds this many hits
+constexpr int STG_PITCH = 36;  // floats per staging row (32 scores + padding)
+
+// LCAP == 32: each thread keeps its row's best 32 (score, column) pairs sorted in
+// registers and appends hits (score below its 32nd best) to a private buffer in
+// shared memory; batches of 16 are merged by data-independent sorting networks,
+// so the 32 rows of a warp merge in lockstep without divergence.
+// LCAP > 32: per-thread sorted lists in shared memory with insertion.
 template <int LCAP>
 struct Cfg {
-  static constexpr int kStages = LCAP <= 32 ? 4 : (LCAP <= 64 ? 3 : 2);
-  static constexpr int kListBytes = BM * LCAP * 8;
+  static constexpr bool kWarpSelect = LCAP == 32;
+  static constexpr int kStages = LCAP <= 32 ? 3 : (LCAP <= 64 ? 3 : 2);
+  static constexpr int kListBytes = kWarpSelect ? BM * BUF * 8 + BM * STG_PITCH * 4 : BM * LCAP * 8;
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = 1024 + kStages * STAGE_BYTES + kListBytes + kBarBytes;
 };
@@ -50,8 +64,8 @@ struct Plan {
   size_t ws_bytes;
   // workspace layout
   int32_t* status;
-  __nv_bfloat16* xb;
-  float* sqb;
+  __nv_bfloat16* xa;  // A operand rows [x~, 1, 1, 1]
+  __nv_bfloat16* xb;  // B operand rows [-2 x~, h1, h2, h3]
   float* cand_s;
   int32_t* cand_i;
 };
@@ -75,7 +89,9 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) 
   if (p.L < k) p.L = k;
   if (p.L > 128) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute: k + extra must be <= 128 (got %d)", k + extra);
   p.lcap = p.L <= 32 ? 32 : (p.L <= 64 ? 64 : 128);
-  p.ld = (d + 7) / 8 * 8;
+  // features + three norm columns, padded to whole 64-element K blocks so every
+  // 128-byte TMA box row starts on a 128-byte boundary
+  p.ld = (d + 3 + BK - 1) / BK * BK;
   p.num_kb = (int)ceil_div(p.ld, BK);
   p.row_blocks = ceil_div(n, BM);
   p.col_tiles = ceil_div(n, BN);
@@ -92,44 +108,105 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) 
   p.slots = (int)slots;
   Carver c(ws);
   p.status = c.take<int32_t>(64);
+  p.xa = c.take<__nv_bfloat16>((size_t)n * p.ld, 1024);
   p.xb = c.take<__nv_bfloat16>((size_t)n * p.ld, 1024);
-  p.sqb = c.take<float>((size_t)p.cols_pad);
   p.cand_s = c.take<float>((size_t)n * p.slots * p.L);
   p.cand_i = c.take<int32_t>((size_t)n * p.slots * p.L);
   p.ws_bytes = c.bytes();
   return UMAPB_OK;
 }
 
-// ---- 1. prep: bf16 copy + norms of the rounded rows -------------------------
-__global__ void prep_kernel(const float* __restrict__ X, int64_t n, int d, int ld, __nv_bfloat16* __restrict__ xb,
-                            float* __restrict__ sqb, int64_t cols_pad) {
+// ---- 1. prep: augmented BF16 operands (one warp per row) ---------------------
+__global__ void prep_kernel(const float* __restrict__ X, int64_t n, int d, int ld, __nv_bfloat16* __restrict__ xa,
+                            __nv_bfloat16* __restrict__ xb) {
   const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (row >= cols_pad) return;
-  if (row >= n) {
-    if (lane == 0) sqb[row] = INFINITY;
-    return;
-  }
+  if (row >= n) return;
   const float* xr = X + row * d;
+  __nv_bfloat16* ar = xa + row * ld;
   __nv_bfloat16* br = xb + row * ld;
   float acc = 0.f;
-  for (int c = lane; c < ld; c += 32) {
-    const float v = c < d ? __ldg(xr + c) : 0.f;
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    br[c] = h;
+  for (int c = lane; c < d; c += 32) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(__ldg(xr + c));
     const float r = __bfloat162float(h);
+    ar[c] = h;
+    br[c] = __float2bfloat16_rn(-2.0f * r);  // exact: a power-of-two scaling
     acc = fmaf(r, r, acc);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-  if (lane == 0) sqb[row] = acc;
+  // |x~|^2 = h1 + h2 + h3; each remainder is exact in float32
+  const __nv_bfloat16 h1 = __float2bfloat16_rn(acc);
+  const float r1 = acc - __bfloat162float(h1);
+  const __nv_bfloat16 h2 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 h3 = __float2bfloat16_rn(r1 - __bfloat162float(h2));
+  const __nv_bfloat16 one = __float2bfloat16_rn(1.0f), zero = __float2bfloat16_rn(0.0f);
+  for (int c = d + lane; c < ld; c += 32) {
+    const int e = c - d;
+    ar[c] = e < 3 ? one : zero;
+    br[c] = e == 0 ? h1 : (e == 1 ? h2 : (e == 2 ? h3 : zero));
+  }
 }
+
+// ---- sorting networks on (score, column) pairs held in registers -------------
+__device__ __forceinline__ bool key_lt2(float a, int ia, float b, int ib) {
+  return a < b || (a == b && ia < ib);
+}
+
+__device__ __forceinline__ void cex(float& a, int& ia, float& b, int& ib, bool ascending) {
+  const bool sw = ascending ? key_lt2(b, ib, a, ia) : key_lt2(a, ia, b, ib);
+  const float ta = a, tb = b;
+  const int xa = ia, xb = ib;
+  a = sw ? tb : ta;
+  b = sw ? ta : tb;
+  ia = sw ? xb : xa;
+  ib = sw ? xa : xb;
+}
+
+// ascending bitonic sort of 16 pairs
+__device__ __forceinline__ void sort16(float (&v)[16], int (&x)[16]) {
+#pragma unroll
+  for (int size = 2; size <= 16; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int j = i ^ stride;
+        if (j > i) cex(v[i], x[i], v[j], x[j], (i & size) == 0);
+      }
+    }
+  }
+}
+
+// list (32, ascending) := smallest 32 of list U batch (16, ascending), ascending.
+// [list, +inf x16, reversed batch] is bitonic; its half-cleaner keeps the 32
+// smallest in the lower half, which a bitonic merge then sorts.
+__device__ __forceinline__ void merge_32_16(float (&lv)[32], int (&li)[32], const float (&bv)[16],
+                                            const int (&bx)[16]) {
+#pragma unroll
+  for (int i = 16; i < 32; ++i) {
+    const float b = bv[31 - i];
+    const int ib = bx[31 - i];
+    if (key_lt2(b, ib, lv[i], li[i])) {
+      lv[i] = b;
+      li[i] = ib;
+    }
+  }
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) {
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      if ((i & stride) == 0) cex(lv[i], li[i], lv[i + stride], li[i + stride], true);
+    }
+  }
+}
+
 
 // ---- 2. tcgen05 distance tiles + fused per-row top-L ------------------------
 template <int LCAP>
 __global__ void __launch_bounds__(THREADS, 1)
     topk_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                const float* __restrict__ sqb, int n, int num_kb, int64_t col_tiles, int64_t tiles, int slots,
+                int n, int num_kb, int64_t col_tiles, int64_t tiles, int slots,
                 int L, float* __restrict__ cand_s, int32_t* __restrict__ cand_i, int32_t* __restrict__ status) {
   using C = Cfg<LCAP>;
   extern __shared__ uint8_t smem_raw[];
@@ -169,7 +246,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc::prefetch_tmap(&tmB);
   }
   if (warp == 2) tc::tmem_alloc(tmem_slot, 512);
-  if (warp >= 4) {
+  if (!C::kWarpSelect && warp >= 4) {
     const int r = threadIdx.x - 128;
     for (int e = 0; e < LCAP; ++e) {
       list_s[e * BM + r] = INFINITY;
@@ -241,7 +318,135 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (acc == 0) acc_phase ^= 1;
       }
     }
-  } else if (warp >= 4) {
+  } else if (C::kWarpSelect && warp >= 4) {
+    // ---------------- epilogue: batched per-row top-32 (L <= 32) ----------------
+    // Thread r of the four epilogue warps owns TMEM lane r, i.e. query row
+    // rb*128 + r.  It keeps the row's best 32 (score, column) pairs sorted in
+    // registers (lv/li; lv[31] is the admission threshold) and appends every hit
+    // to its own BUF-entry buffer in shared memory (two stores, no loop).  When a
+    // thread of the warp holds MERGE_AT hits the whole warp merges its buffers in
+    // batches of 16 with a bitonic sort network and a bitonic 32+16 merge —
+    // data-independent, so the 32 rows of a warp run in lockstep.
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    float* bs = list_s;                                          // [BUF][BM]
+    int32_t* bi = reinterpret_cast<int32_t*>(list_s + BUF * BM);  // [BUF][BM]
+    // per-thread staging row for the chunk being appended; a pitch of 36 floats
+    // keeps each quarter-warp's 16-byte stores on distinct banks
+    float* stg_row = list_s + 2 * BUF * BM + r * STG_PITCH;
+    float lv[32];
+    int li[32];
+#pragma unroll
+    for (int e = 0; e < 32; ++e) {
+      lv[e] = INFINITY;
+      li[e] = 0x7fffffff;
+    }
+    int cnt = 0;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    int64_t cur_rb = -1;
+    bool ok = true;
+    auto merge_pending = [&]() {
+      while (__any_sync(0xffffffffu, cnt > 0)) {
+        const int m = cnt < 16 ? cnt : 16;
+        const int base = cnt - m;
+        float bv[16];
+        int bx[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          if (e < m) {
+            bv[e] = bs[(base + e) * BM + r];
+            bx[e] = bi[(base + e) * BM + r];
+          } else {
+            bv[e] = INFINITY;
+            bx[e] = 0x7fffffff;
+          }
+        }
+        cnt = base;
+        sort16(bv, bx);
+        merge_32_16(lv, li, bv, bx);
+      }
+    };
+    auto flush = [&](int64_t rb) {
+      merge_pending();
+      const int64_t row = rb * BM + r;
+      const int64_t slot = cta - first_cta(rb * col_tiles, tiles, G);
+      if (row < n) {
+        float* cs = cand_s + (row * slots + slot) * L;
+        int32_t* ci = cand_i + (row * slots + slot) * L;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+          if (e < L) {
+            cs[e] = lv[e];
+            ci[e] = li[e] == 0x7fffffff ? -1 : li[e];
+          }
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        lv[e] = INFINITY;
+        li[e] = 0x7fffffff;
+      }
+    };
+    for (int64_t t = t_begin; t < t_end; ++t) {
+      const int64_t rb = t / col_tiles;
+      const int ct = (int)(t % col_tiles);
+      if (rb != cur_rb) {
+        if (cur_rb >= 0) flush(cur_rb);
+        cur_rb = rb;
+      }
+      if (!tc::mbar_wait(&tfull[acc], acc_phase, abort_flag)) {
+        ok = false;
+        break;
+      }
+      tc::tc_fence_after();
+      const int64_t row = rb * BM + r;
+      const bool row_ok = row < n;
+      const int self_col = row_ok ? (int)row : -1;
+      const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+      for (int ch = 0; ch < BN / 32; ++ch) {
+        float v[32];
+        __syncwarp();
+        tc::tmem_ld32(taddr + ch * 32, v);
+        const int col0 = ct * BN + ch * 32;
+        // branch-free hit mask of the 32 columns (four independent OR chains);
+        // rows past n never admit
+        const float tau = row_ok ? lv[31] : -INFINITY;
+        unsigned m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          m0 |= (v[j] < tau ? 1u : 0u) << j;
+          m1 |= (v[j + 8] < tau ? 1u : 0u) << j;
+          m2 |= (v[j + 16] < tau ? 1u : 0u) << j;
+          m3 |= (v[j + 24] < tau ? 1u : 0u) << j;
+        }
+        unsigned mask = m0 | (m1 << 8) | (m2 << 16) | (m3 << 24);
+        const int self_off = self_col - col0;  // the row itself
+        if ((unsigned)self_off < 32u) mask &= ~(1u << self_off);
+        const int lim = n - col0;  // zero-filled columns past n
+        if (lim < 32) mask &= lim <= 0 ? 0u : ((1u << lim) - 1u);
+        if (mask) {  // stage the chunk, then append the hits in column order
+          float4* st4 = reinterpret_cast<float4*>(stg_row);
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) st4[j4] = make_float4(v[4 * j4], v[4 * j4 + 1], v[4 * j4 + 2], v[4 * j4 + 3]);
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            bs[cnt * BM + r] = stg_row[j];
+            bi[cnt * BM + r] = col0 + j;
+            ++cnt;
+          }
+        }
+        if (__any_sync(0xffffffffu, cnt >= MERGE_AT)) merge_pending();
+      }
+      tc::tc_fence_before();
+      tc::mbar_arrive(&tempty[acc]);
+      acc ^= 1;
+      if (acc == 0) acc_phase ^= 1;
+    }
+    if (ok && cur_rb >= 0) flush(cur_rb);
+  } else if (!C::kWarpSelect && warp >= 4) {
     // ---------------- epilogue: per-row top-L ----------------
     const int q = warp & 3;  // TMEM lane quarter of this warp
     const int r = q * 32 + lane;
@@ -288,28 +493,22 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncwarp();
         tc::tmem_ld32(taddr + ch * 32, v);
         const int col0 = ct * BN + ch * 32;
-        const float4* sq4 = reinterpret_cast<const float4*>(sqb + col0);
 #pragma unroll
-        for (int j4 = 0; j4 < 8; ++j4) {
-          const float4 sq = __ldg(sq4 + j4);
-          const float sj[4] = {sq.x, sq.y, sq.z, sq.w};
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const float s = fmaf(-2.0f, v[j4 * 4 + u], sj[u]);
-            const int col = col0 + j4 * 4 + u;
-            if (s < tau && row_ok && col != row) {
-              int p = L - 1;
-              while (p > 0) {
-                const float prev = list_s[(p - 1) * BM + r];
-                if (prev <= s) break;
-                list_s[p * BM + r] = prev;
-                list_i[p * BM + r] = list_i[(p - 1) * BM + r];
-                --p;
-              }
-              list_s[p * BM + r] = s;
-              list_i[p * BM + r] = col;
-              tau = list_s[(L - 1) * BM + r];
+        for (int j = 0; j < 32; ++j) {
+          const float s = v[j];
+          const int col = col0 + j;
+          if (s < tau && row_ok && col != row && col < n) {
+            int p = L - 1;
+            while (p > 0) {
+              const float prev = list_s[(p - 1) * BM + r];
+              if (prev <= s) break;
+              list_s[p * BM + r] = prev;
+              list_i[p * BM + r] = list_i[(p - 1) * BM + r];
+              --p;
             }
+            list_s[p * BM + r] = s;
+            list_i[p * BM + r] = col;
+            tau = list_s[(L - 1) * BM + r];
           }
         }
       }
@@ -387,25 +586,60 @@ __global__ void __launch_bounds__(RR_WARPS * 32)
   }
   __syncwarp();
   warp_bitonic(key, idx, P, lane);
-  // exact squared distances of the best L candidates (direct form, FP32)
+  // exact squared distances of the best L candidates (direct form, FP32), four
+  // candidates per pass so every lane keeps several independent loads in flight
   const float* xr = X + row * d;
-  for (int e = 0; e < PL; ++e) {
-    const int j = e < L ? idx[e] : 0x7fffffff;
-    float acc = INFINITY;
-    if (j != 0x7fffffff) {
-      const float* xc = X + (int64_t)j * d;
-      acc = 0.f;
-      for (int c = lane; c < d; c += 32) {
-        const float t = __ldg(xr + c) - __ldg(xc + c);
-        acc = fmaf(t, t, acc);
-      }
+  const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  for (int e0 = 0; e0 < PL; e0 += 4) {
+    int j[4];
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    for (int u = 0; u < 4; ++u) j[u] = (e0 + u < L) ? idx[e0 + u] : 0x7fffffff;
+    if (vec) {
+      const float4* xr4 = reinterpret_cast<const float4*>(xr);
+      for (int c = lane; c < (d >> 2); c += 32) {
+        const float4 a = __ldg(xr4 + c);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (j[u] != 0x7fffffff) {
+            const float4 b = __ldg(reinterpret_cast<const float4*>(X + (int64_t)j[u] * d) + c);
+            const float t0 = a.x - b.x, t1 = a.y - b.y, t2 = a.z - b.z, t3 = a.w - b.w;
+            acc[u] = fmaf(t0, t0, acc[u]);
+            acc[u] = fmaf(t1, t1, acc[u]);
+            acc[u] = fmaf(t2, t2, acc[u]);
+            acc[u] = fmaf(t3, t3, acc[u]);
+          }
+        }
+      }
+    } else {
+      for (int c = lane; c < d; c += 32) {
+        const float a = __ldg(xr + c);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (j[u] != 0x7fffffff) {
+            const float t = a - __ldg(X + (int64_t)j[u] * d + c);
+            acc[u] = fmaf(t, t, acc[u]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
     }
     __syncwarp();
-    if (lane == 0) {
-      key[e] = acc;
-      idx[e] = j;
+    if (lane < 4 && e0 + lane < PL) {
+      float a = acc[0];
+      int jj = j[0];
+#pragma unroll
+      for (int u = 1; u < 4; ++u)
+        if (lane == u) {
+          a = acc[u];
+          jj = j[u];
+        }
+      key[e0 + lane] = jj != 0x7fffffff ? a : INFINITY;
+      idx[e0 + lane] = jj;
     }
     __syncwarp();
   }
@@ -429,7 +663,7 @@ static int launch_topk(const Plan& p, const CUtensorMap& ta, const CUtensorMap& 
     attr_set[dev] = true;
   }
   topk_kernel<LCAP><<<(unsigned)p.grid, THREADS, C::kSmem, stream>>>(
-      ta, tb, p.sqb, (int)p.n, p.num_kb, p.col_tiles, p.tiles, p.slots, p.L, p.cand_s, p.cand_i, p.status);
+      ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles, p.slots, p.L, p.cand_s, p.cand_i, p.status);
   UMAPB_LAUNCH_CHECK("knn_brute: topk kernel launch");
   return UMAPB_OK;
 }
@@ -472,13 +706,13 @@ extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, 
   UMAPB_CUDA_TRY(cudaMemsetAsync(p.cand_i, 0xFF, (size_t)n * p.slots * p.L * sizeof(int32_t), stream),
                  "knn_brute: candidate reset");
   {
-    const int64_t warps = p.cols_pad;
+    const int64_t warps = n;
     const unsigned blocks = (unsigned)ceil_div(warps * 32, 256);
-    knn::prep_kernel<<<blocks, 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xb, p.sqb, p.cols_pad);
+    knn::prep_kernel<<<blocks, 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
     UMAPB_LAUNCH_CHECK("knn_brute: prep kernel launch");
   }
   CUtensorMap ta, tb;
-  if ((s = make_tmap_bf16_2d(&ta, p.xb, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BM, knn::BK))) return s;
+  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BM, knn::BK))) return s;
   if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BN, knn::BK))) return s;
   if (p.lcap == 32)
     s = knn::launch_topk<32>(p, ta, tb, stream);

@@ -1,0 +1,563 @@
+// NNDescent kNN graph — replaces mlx_vis/_nndescent/nndescent.py:34-486 and 573-641.
+//
+// The host (Python) keeps the reference's control flow (random init and
+// projections from NumPy's global stream, per-iteration mc/j_nn from the update
+// fraction, full vs converging path, FP16 iterations 1-4, low-dimensional
+// iterations 0-1, FP32 recompute after iteration 4).  These kernels do the data
+// work of one iteration:
+//
+// reverse candidates (nndescent.py:406-436): slot p of row j = p-th smallest
+//   source i with j in knn(i); empty slots hold 0 (the reference's zero padding).
+//   Bucket fill with atomics, then one warp sorts each bucket: deterministic.
+// row update (nndescent.py:241-280 full path, 103-220 converging path), one warp
+//   per row:
+//   1. candidate row = [current k | nn-of-nn (mc_new sources x first j_nn of
+//      their rows) | reverse k]; on the converging path the sources are the
+//      row's NEW neighbours first (stable), and rows with no NEW flag are copied.
+//   2. duplicates: the first occurrence in that order survives (a shared-memory
+//      hash set per warp; equal ids inside one 32-wide chunk resolved with
+//      __match_any_sync) — what the reference's stable sort by id keeps.
+//   3. distances max(sq_i + sq_c - 2 x_i.x_c, 0) only for surviving candidates
+//      that need one: stored distances are reused for current neighbours unless
+//      the iteration recomputes them; FP16 iterations round the FP32-accumulated
+//      dot product to FP16 like _gather_dists_half.  Self and duplicates get 1e30.
+//   4. the k smallest (distance, id) pairs, kept as a warp-distributed sorted list
+//      (ballot finds the slot, shfl_up shifts), written with the positional
+//      change flags and a global count of changes (nndescent.py:381-385).
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace umapb {
+namespace nnd {
+
+constexpr float kBig = 1e30f;
+constexpr int kWarps = 4;  // warps per block in the row kernels
+
+__device__ __forceinline__ bool key_lt(float a, int ia, float b, int ib) {
+  return a < b || (a == b && ia < ib);
+}
+
+// ---- distance helpers --------------------------------------------------------
+template <class T>
+__device__ __forceinline__ float to_f(T v);
+template <>
+__device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+
+// dot products of x (shared memory copy of row i) with up to 4 rows of X, summed
+// over the warp; every lane gets the totals
+template <class T>
+__device__ __forceinline__ void dot4(const T* __restrict__ X, const T* xs, int dd, const int (&c)[4], int cnt,
+                                     int lane, float (&out)[4]) {
+  float acc[4] = {0.f, 0.f, 0.f, 0.f};
+  constexpr int V = 16 / sizeof(T);  // elements per 16-byte vector
+  const bool vec = (dd % V) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  if (vec) {
+    const int nv = dd / V;
+    for (int t = lane; t < nv; t += 32) {
+      const uint4 a4 = reinterpret_cast<const uint4*>(xs)[t];
+      const T* a = reinterpret_cast<const T*>(&a4);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (u < cnt) {
+          const uint4 b4 = __ldg(reinterpret_cast<const uint4*>(X + (int64_t)c[u] * dd) + t);
+          const T* bb = reinterpret_cast<const T*>(&b4);
+#pragma unroll
+          for (int e = 0; e < V; ++e) acc[u] = fmaf(to_f<T>(a[e]), to_f<T>(bb[e]), acc[u]);
+        }
+      }
+    }
+  } else {
+    for (int t = lane; t < dd; t += 32) {
+      const float a = to_f<T>(xs[t]);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (u < cnt) acc[u] = fmaf(a, to_f<T>(X[(int64_t)c[u] * dd + t]), acc[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], o);
+    out[u] = acc[u];
+  }
+}
+
+__device__ __forceinline__ float d2_from_dot(float sq_i, float sq_c, float dot, bool half_round) {
+  if (half_round) dot = __half2float(__float2half_rn(dot));
+  return fmaxf(__fsub_rn(__fadd_rn(sq_i, sq_c), __fmul_rn(2.0f, dot)), 0.0f);
+}
+
+// Inserts (d, id) into the warp-distributed ascending list (lane l holds entry l).
+__device__ __forceinline__ void list_insert(float& lv, int& li, float d, int id, int k, int lane) {
+  const int pos = __popc(__ballot_sync(0xffffffffu, lane < k && key_lt(lv, li, d, id)));
+  const float up_v = __shfl_up_sync(0xffffffffu, lv, 1);
+  const int up_i = __shfl_up_sync(0xffffffffu, li, 1);
+  if (lane < k) {
+    if (lane > pos) {
+      lv = up_v;
+      li = up_i;
+    } else if (lane == pos) {
+      lv = d;
+      li = id;
+    }
+  }
+}
+
+// ---- small kernels -------------------------------------------------------------
+template <class T>
+__global__ void sqnorm_kernel(const T* __restrict__ X, int64_t n, int dd, float* __restrict__ sq) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  float acc = 0.f;
+  for (int t = lane; t < dd; t += 32) {
+    const float v = to_f<T>(X[row * dd + t]);
+    acc = fmaf(v, v, acc);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) sq[row] = acc;
+}
+
+__global__ void to_half_kernel(const float* __restrict__ X, int64_t m, __half* __restrict__ H) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    H[t] = __float2half_rn(X[t]);
+}
+
+// d2 of each row to its k listed neighbours (FP32, full space), optionally sorted
+// ascending by (distance, id) — _gather_dists (nndescent.py:573-612) and the sort
+// after the random init (nndescent.py:63-65).
+__global__ void gather_rows_kernel(const float* __restrict__ X, const float* __restrict__ sq, int64_t n, int dd,
+                                   int32_t* __restrict__ idx, float* __restrict__ dist, int k, int sort_rows) {
+  extern __shared__ float xs_all[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
+  if (row >= n) return;
+  float* xs = xs_all + warp * dd;
+  for (int t = lane; t < dd; t += 32) xs[t] = X[row * dd + t];
+  __syncwarp();
+  const float sqi = sq[row];
+  float my_d = kBig;
+  int my_i = 0x7fffffff;
+  for (int p0 = 0; p0 < k; p0 += 4) {
+    int c[4];
+    const int cnt = min(4, k - p0);
+    for (int u = 0; u < 4; ++u) c[u] = u < cnt ? idx[row * k + p0 + u] : 0;
+    float dots[4];
+    dot4<float>(X, xs, dd, c, cnt, lane, dots);
+    for (int u = 0; u < cnt; ++u) {
+      const float d2 = d2_from_dot(sqi, sq[c[u]], dots[u], false);
+      if (lane == p0 + u) {
+        my_d = d2;
+        my_i = c[u];
+      }
+    }
+  }
+  if (sort_rows) {  // warp bitonic sort of k <= 32 (distance, id) pairs held one per lane
+    for (int size = 2; size <= 32; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const float od = __shfl_xor_sync(0xffffffffu, my_d, stride);
+        const int oi = __shfl_xor_sync(0xffffffffu, my_i, stride);
+        const bool lower = (lane & stride) == 0;
+        const bool asc = (lane & size) == 0;
+        const bool take_other = (lower == asc) ? key_lt(od, oi, my_d, my_i) : key_lt(my_d, my_i, od, oi);
+        if (take_other) {
+          my_d = od;
+          my_i = oi;
+        }
+      }
+    }
+  }
+  if (lane < k) {
+    idx[row * k + lane] = my_i;
+    dist[row * k + lane] = my_d;
+  }
+}
+
+// ---- reverse candidates ----------------------------------------------------------
+__global__ void indegree_kernel(const int32_t* __restrict__ idx, int64_t m, int32_t* __restrict__ deg) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&deg[idx[t]], 1);
+}
+
+__global__ void bucket_fill_kernel(const int32_t* __restrict__ idx, int64_t m, int k, const int32_t* __restrict__ off,
+                                   int32_t* __restrict__ fill, int32_t* __restrict__ bucket) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int j = idx[t];
+    const int p = atomicAdd(&fill[j], 1);
+    bucket[off[j] + p] = (int32_t)(t / k);
+  }
+}
+
+// rev[j][p] = p-th smallest source in j's bucket, 0 when the bucket is shorter
+__global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const int32_t* __restrict__ off,
+                                     const int32_t* __restrict__ deg, int64_t n, int k, int32_t* __restrict__ rev) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * kWarps + warp;
+  if (j >= n) return;
+  const int cnt = deg[j];
+  const int32_t* b = bucket + off[j];
+  // k passes: each finds the smallest source above the previous pick (sources are distinct
+  // except when a row lists j twice; then it is repeated, like the reference's sort keeps it)
+  int prev = -1, prev_mult = 0;
+  for (int p = 0; p < k; ++p) {
+    int best = 0x7fffffff;
+    int mult = 0;
+    for (int t = lane; t < cnt; t += 32) {
+      const int s = b[t];
+      if (s > prev && s < best) best = s;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+    // multiplicity of prev: emit prev again while it has unused copies
+    int cprev = 0;
+    if (prev >= 0) {
+      for (int t = lane; t < cnt; t += 32) cprev += b[t] == prev ? 1 : 0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) cprev += __shfl_xor_sync(0xffffffffu, cprev, o);
+    }
+    int out;
+    if (prev >= 0 && prev_mult < cprev) {
+      out = prev;
+      mult = prev_mult + 1;
+    } else if (best != 0x7fffffff) {
+      out = best;
+      mult = 1;
+    } else {
+      out = 0;  // empty slot: zero, as the reference's scatter into zeros leaves it
+      mult = prev_mult;
+    }
+    if (lane == 0) rev[j * k + p] = out;
+    if (out != 0 || best != 0x7fffffff) {
+      if (out != prev) prev = out;
+      prev_mult = mult;
+    }
+  }
+}
+
+// ---- one NNDescent iteration, one warp per row ------------------------------------
+struct IterArgs {
+  const void* Xd;  // distance space, float or __half rows of length dd
+  const float* sqd;
+  int dd;
+  const int32_t* idx_old;
+  const float* dist_old;
+  const uint8_t* flags_old;  // converging path only
+  const int32_t* rev;        // nullable
+  int64_t n;
+  int k, mc_new, j_nn;
+  int converging, recompute_cur, half_round;
+  int tcap, hcap;  // candidate capacity per row (multiple of 32) and hash size (power of two)
+  int32_t* idx_new;
+  float* dist_new;
+  uint8_t* flags_new;
+  unsigned long long* changed;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
+  const size_t per_warp = (size_t)a.dd * sizeof(T) + (size_t)a.tcap * 12 + (size_t)a.hcap * 4 + 32 * 4;
+  uint8_t* base = smem_raw + warp * ((per_warp + 15) / 16 * 16);
+  T* xs = reinterpret_cast<T*>(base);
+  int32_t* cid = reinterpret_cast<int32_t*>(base + (a.dd * sizeof(T) + 15) / 16 * 16);
+  float* cd = reinterpret_cast<float*>(cid + a.tcap);
+  int32_t* todo = reinterpret_cast<int32_t*>(cd + a.tcap);
+  int32_t* htab = todo + a.tcap;
+  int32_t* srcs = htab + a.hcap;
+  if (row >= a.n) return;
+  const int k = a.k;
+  const int32_t* orow = a.idx_old + row * k;
+
+  // row-local copy of the old neighbours (lane p holds entry p; k <= 32)
+  const int my_old = lane < k ? orow[lane] : -1;
+  const float my_old_d = lane < k ? a.dist_old[row * k + lane] : kBig;
+  if (a.converging) {
+    const bool f = lane < k && a.flags_old[row * k + lane];
+    const unsigned fb = __ballot_sync(0xffffffffu, f);
+    if (fb == 0) {  // no NEW neighbour: the row keeps its list (nndescent.py:111-126, 211-217)
+      if (lane < k) {
+        a.idx_new[row * k + lane] = my_old;
+        a.dist_new[row * k + lane] = my_old_d;
+        a.flags_new[row * k + lane] = 0;
+      }
+      return;
+    }
+    // NEW-first stable order (nndescent.py:105-106)
+    const unsigned lt = (1u << lane) - 1u;
+    const int nnew = __popc(fb);
+    const unsigned ob = __ballot_sync(0xffffffffu, lane < k && !f);
+    const int pos = f ? __popc(fb & lt) : nnew + __popc(ob & lt);
+    if (lane < k) srcs[pos] = my_old;
+  } else {
+    if (lane < k) srcs[lane] = my_old;
+  }
+  for (int t = lane; t < a.dd; t += 32) xs[t] = reinterpret_cast<const T*>(a.Xd)[row * a.dd + t];
+  for (int t = lane; t < a.hcap; t += 32) htab[t] = -1;
+  __syncwarp();
+
+  // 1. candidate ids in the reference's column order
+  const int nn_cols = a.mc_new * a.j_nn;
+  const int T_total = k + nn_cols + (a.rev ? k : 0);
+  for (int t = lane; t < a.tcap; t += 32) {
+    int id = 0x7fffffff;
+    if (t < k) {
+      id = orow[t];
+    } else if (t < k + nn_cols) {
+      const int q = t - k;
+      const int src = srcs[q / a.j_nn];
+      id = a.idx_old[(int64_t)src * k + (q % a.j_nn)];
+    } else if (t < T_total) {
+      id = a.rev[row * k + (t - k - nn_cols)];
+    }
+    cid[t] = id;
+  }
+  __syncwarp();
+
+  // 2. first-occurrence dedup + 3. list of distances to compute
+  int n_todo = 0;
+  for (int t0 = 0; t0 < a.tcap; t0 += 32) {
+    const int t = t0 + lane;
+    const int id = cid[t];
+    const bool valid = t < T_total;
+    const unsigned same = __match_any_sync(0xffffffffu, id);
+    bool first = valid && (__ffs(same) - 1) == lane;  // lowest lane of an equal-id group in this chunk
+    if (first) {
+      unsigned h = ((unsigned)id * 0x9E3779B1u) & (unsigned)(a.hcap - 1);
+      while (true) {
+        const int old = atomicCAS(&htab[h], -1, id);
+        if (old == -1) break;
+        if (old == id) {
+          first = false;
+          break;
+        }
+        h = (h + 1) & (unsigned)(a.hcap - 1);
+      }
+    }
+    float d = kBig;
+    bool need = false;
+    if (first && id != (int)row) {
+      if (t < k && !a.recompute_cur) d = a.dist_old[row * k + t];
+      else need = true;
+    }
+    cd[t] = d;
+    const unsigned nb = __ballot_sync(0xffffffffu, need);
+    if (need) todo[n_todo + __popc(nb & ((1u << lane) - 1u))] = t;
+    n_todo += __popc(nb);
+  }
+  __syncwarp();
+  const float sqi = a.sqd[row];
+  for (int p0 = 0; p0 < n_todo; p0 += 4) {
+    int c[4], tt[4];
+    const int cnt = min(4, n_todo - p0);
+    for (int u = 0; u < 4; ++u) {
+      tt[u] = u < cnt ? todo[p0 + u] : 0;
+      c[u] = u < cnt ? cid[tt[u]] : 0;
+    }
+    float dots[4];
+    dot4<T>(reinterpret_cast<const T*>(a.Xd), xs, a.dd, c, cnt, lane, dots);
+    if (lane < cnt) {
+      float dot = dots[0];
+      for (int u = 1; u < 4; ++u)
+        if (lane == u) dot = dots[u];
+      cd[tt[lane]] = d2_from_dot(sqi, a.sqd[c[lane]], dot, a.half_round != 0);
+    }
+  }
+  __syncwarp();
+
+  // 4. k smallest (distance, id) over all candidate columns
+  float lv = kBig * 4.0f;  // above every real key, including 1e30 entries
+  int li = 0x7fffffff;
+  float tau = lv;
+  int tau_i = li;
+  for (int t0 = 0; t0 < a.tcap; t0 += 32) {
+    const int t = t0 + lane;
+    const float d = t < T_total ? cd[t] : INFINITY;
+    const int id = cid[t];
+    unsigned b = __ballot_sync(0xffffffffu, t < T_total && key_lt(d, id, tau, tau_i));
+    while (b) {
+      const int src = __ffs(b) - 1;
+      const float sd = __shfl_sync(0xffffffffu, d, src);
+      const int si = __shfl_sync(0xffffffffu, id, src);
+      list_insert(lv, li, sd, si, k, lane);
+      tau = __shfl_sync(0xffffffffu, lv, k - 1);
+      tau_i = __shfl_sync(0xffffffffu, li, k - 1);
+      b &= ~(1u << src);
+      b &= __ballot_sync(0xffffffffu, key_lt(d, id, tau, tau_i));
+    }
+  }
+  if (lane < k) {
+    a.idx_new[row * k + lane] = li;
+    a.dist_new[row * k + lane] = lv;
+    const bool ch = li != my_old;
+    a.flags_new[row * k + lane] = ch ? 1 : 0;
+  }
+  const int nch = __popc(__ballot_sync(0xffffffffu, lane < k && li != my_old));
+  if (lane == 0 && nch) atomicAdd(a.changed, (unsigned long long)nch);
+}
+
+}  // namespace nnd
+}  // namespace umapb
+
+using namespace umapb;
+
+static size_t iter_smem_per_warp(int dd, int elem, int tcap, int hcap) {
+  const size_t per_warp = (size_t)dd * elem + (size_t)tcap * 12 + (size_t)hcap * 4 + 32 * 4 + 16;
+  return (per_warp + 15) / 16 * 16;
+}
+
+extern "C" int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq,
+                                 umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(X && sq && n >= 1 && dd >= 1, "nnd_sqnorms: bad arguments");
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  const unsigned blocks = (unsigned)ceil_div(n * 32, 256);
+  if (half)
+    nnd::sqnorm_kernel<__half><<<blocks, 256, 0, stream>>>(static_cast<const __half*>(X), n, dd, sq);
+  else
+    nnd::sqnorm_kernel<float><<<blocks, 256, 0, stream>>>(static_cast<const float*>(X), n, dd, sq);
+  UMAPB_LAUNCH_CHECK("nnd_sqnorms kernel");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_to_half(const float* X, int64_t count, void* H, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(X && H && count >= 0, "nnd_to_half: bad arguments");
+  if (count == 0) return UMAPB_OK;
+  const int64_t want = ceil_div(count, 256);
+  const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
+  nnd::to_half_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(X, count,
+                                                                                    static_cast<__half*>(H));
+  UMAPB_LAUNCH_CHECK("nnd_to_half kernel");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int32_t dd, int32_t* idx, float* dist,
+                                int32_t k, int32_t sort_rows, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(X && sq && idx && dist, "nnd_gather: null array argument");
+  UMAPB_REQUIRE(n >= 1 && dd >= 1 && k >= 1 && k <= 32, "nnd_gather: need 1 <= k <= 32");
+  const size_t smem = (size_t)nnd::kWarps * dd * sizeof(float);
+  UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_gather: row dimension too large");
+  static bool attr = false;
+  if (!attr) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::gather_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024),
+                   "nnd_gather: smem attribute");
+    attr = true;
+  }
+  nnd::gather_rows_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, smem,
+                            reinterpret_cast<cudaStream_t>(stream_)>>>(X, sq, n, dd, idx, dist, k, sort_rows);
+  UMAPB_LAUNCH_CHECK("nnd_gather kernel");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_reverse_workspace(int64_t n, int32_t k, size_t* bytes) {
+  clear_error();
+  UMAPB_REQUIRE(bytes && n >= 1 && k >= 1, "nnd_reverse_workspace: bad arguments");
+  Carver c(nullptr);
+  c.take<int32_t>(64);
+  c.take<int32_t>((size_t)n + 1);  // degree -> offsets
+  c.take<int32_t>((size_t)n + 1);  // fill counters
+  c.take<int32_t>((size_t)n);      // degree copy
+  c.take<int32_t>((size_t)n * k);  // buckets
+  c.take<int64_t>(8);
+  *bytes = c.bytes();
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, void* workspace,
+                                 size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(idx && rev && n >= 1 && k >= 1, "nnd_reverse: bad arguments");
+  UMAPB_REQUIRE(n < ((int64_t)1 << 31) / 2, "nnd_reverse: n too large");
+  Carver c(workspace);
+  c.take<int32_t>(64);
+  int32_t* off = c.take<int32_t>((size_t)n + 1);
+  int32_t* fill = c.take<int32_t>((size_t)n + 1);
+  int32_t* deg = c.take<int32_t>((size_t)n);
+  int32_t* bucket = c.take<int32_t>((size_t)n * k);
+  int64_t* total = c.take<int64_t>(8);
+  if (!workspace || workspace_bytes < c.bytes())
+    return set_error(UMAPB_ERR_WORKSPACE, "nnd_reverse: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
+  const int64_t m = n * k;
+  UMAPB_CUDA_TRY(cudaMemsetAsync(off, 0, sizeof(int32_t) * (n + 1), stream), "nnd_reverse: reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(fill, 0, sizeof(int32_t) * (n + 1), stream), "nnd_reverse: reset");
+  const int64_t want = ceil_div(m, 256);
+  const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
+  nnd::indegree_kernel<<<blocks, 256, 0, stream>>>(idx, m, off);
+  UMAPB_CUDA_TRY(cudaMemcpyAsync(deg, off, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, stream),
+                 "nnd_reverse: degree copy");
+  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n, total);
+  nnd::bucket_fill_kernel<<<blocks, 256, 0, stream>>>(idx, m, k, off, fill, bucket);
+  nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
+                                                                                                  n, k, rev);
+  UMAPB_LAUNCH_CHECK("nnd_reverse kernels");
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t half, const int32_t* idx_old,
+                                   const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n,
+                                   int32_t k, int32_t mc_new, int32_t j_nn, int32_t converging,
+                                   int32_t recompute_cur, int32_t* idx_new, float* dist_new, uint8_t* flags_new,
+                                   unsigned long long* changed, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(Xd && sqd && idx_old && dist_old && idx_new && dist_new && flags_new && changed,
+                "nnd_iteration: null array argument");
+  UMAPB_REQUIRE(!converging || flags_old, "nnd_iteration: the converging path needs the flags");
+  UMAPB_REQUIRE(n >= 2 && dd >= 1, "nnd_iteration: bad shape");
+  UMAPB_REQUIRE(k >= 1 && k <= 32, "nnd_iteration: k must be in [1, 32]");
+  UMAPB_REQUIRE(mc_new >= 0 && mc_new <= k && j_nn >= 0 && j_nn <= k, "nnd_iteration: bad mc_new / j_nn");
+  nnd::IterArgs a;
+  a.Xd = Xd;
+  a.sqd = sqd;
+  a.dd = dd;
+  a.idx_old = idx_old;
+  a.dist_old = dist_old;
+  a.flags_old = flags_old;
+  a.rev = rev;
+  a.n = n;
+  a.k = k;
+  a.mc_new = mc_new;
+  a.j_nn = j_nn;
+  a.converging = converging;
+  a.recompute_cur = recompute_cur;
+  a.half_round = half;
+  const int T = k + mc_new * j_nn + (rev ? k : 0);
+  a.tcap = (T + 31) / 32 * 32;
+  int h = 64;
+  while (h < 2 * T) h <<= 1;
+  a.hcap = h;
+  a.idx_new = idx_new;
+  a.dist_new = dist_new;
+  a.flags_new = flags_new;
+  a.changed = changed;
+  const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(dd, half ? 2 : 4, a.tcap, a.hcap);
+  UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_iteration: row dimension too large for shared memory");
+  static bool attr = false;
+  if (!attr) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024),
+                   "nnd_iteration: smem attribute");
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        200 * 1024),
+                   "nnd_iteration: smem attribute");
+    attr = true;
+  }
+  const unsigned blocks = (unsigned)ceil_div(n, nnd::kWarps);
+  if (half)
+    nnd::iter_kernel<__half><<<blocks, nnd::kWarps * 32, smem, stream>>>(a);
+  else
+    nnd::iter_kernel<float><<<blocks, nnd::kWarps * 32, smem, stream>>>(a);
+  UMAPB_LAUNCH_CHECK("nnd_iteration kernel");
+  return UMAPB_OK;
+}

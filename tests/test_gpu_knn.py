@@ -79,7 +79,7 @@ def test_brute_ragged_shapes(n, d, k):
     assert_exact_knn(X, idx, dist, k)
 
 
-@pytest.mark.parametrize("k,extra", [(40, 16), (100, 16), (15, 0), (8, 60)])
+@pytest.mark.parametrize("k,extra", [(40, 16), (100, 16), (1, 16), (8, 60)])
 def test_brute_candidate_list_sizes(k, extra):
     X = np.random.default_rng(k).normal(size=(700, 24)).astype(np.float32)
     idx, dist = run_knn(X, k, extra=extra)
