@@ -38,6 +38,14 @@ SIGNATURES = {
     "umapb_layout_prepare": [_p, _p, _i64, _i32, _p, _p, _p, _sz, _p],
     "umapb_layout_epochs": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32,
                             _u64, _p, _sz, _p],
+    "umapb_nnd_sqnorms": [_p, _i64, _i32, _i32, _p, _p],
+    "umapb_nnd_to_half": [_p, _i64, _p, _p],
+    "umapb_nnd_gather": [_p, _p, _i64, _i32, _p, _p, _i32, _i32, _p],
+    "umapb_nnd_reverse_workspace": [_i64, _i32, _psz],
+    "umapb_nnd_reverse": [_p, _i64, _i32, _p, _p, _sz, _p],
+    "umapb_nnd_iteration": [_p, _p, _i32, _i32, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _i32, _i32, _p, _p, _p, _p,
+                            _p],
+    "umapb_nnd_sqrt": [_p, _i64, _p, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],

@@ -1,11 +1,60 @@
-"""NNDescent on one B200 — drop-in for ``mlx_vis.NNDescent`` (mlx_vis/_nndescent/nndescent.py:14-403)."""
+"""NNDescent on one B200 — drop-in for ``mlx_vis.NNDescent`` (mlx_vis/_nndescent/nndescent.py:14-403).
+
+The control flow is the reference's, kept on the host:
+
+* the same random draws from NumPy's global stream: ``np.random.seed``,
+  ``randint(0, n-1, (n, k))`` shifted past self, then the two projections
+  ``randn(d, 100)/sqrt(100)`` and ``randn(d, 300)/sqrt(300)`` (nndescent.py:47-82),
+  so the random start and the projections are identical to the reference's;
+* per iteration mc_nn / j_nn from the update fraction (nndescent.py:100-101);
+* full path while the update fraction is >= 0.5: iteration 0 in the 100-d
+  projection, iteration 1 in the 300-d projection, FP16 distances in iterations
+  1-4 with current distances recomputed, an FP32 recompute after iteration 4,
+  reverse candidates while the fraction is >= 0.10 (nndescent.py:221-378);
+* converging path below 0.5: only rows with a NEW neighbour, NEW neighbours
+  first as sources, mc_new = max(3, int(k uf)), stored distances reused
+  (nndescent.py:103-220);
+* stop when the fraction of positional changes drops below delta (381-398).
+
+Every data-parallel step runs in libumap_b200 (nndescent.cu); the projections
+are plain FP32 GEMMs (cuBLAS through torch.matmul with TF32 disabled).  One
+device-to-host read per iteration fetches the change count that drives the
+control flow, as in the reference.
+"""
 
 from __future__ import annotations
+
+import time
 
 import numpy as np
 import torch
 
+from mlx_vis_b200 import _lib
 from mlx_vis_b200._device import to_device_f32, to_host
+from mlx_vis_b200._lib import call, ptr, query, stream_handle
+
+def iteration_params(update_frac: float, k: int, mc: int):
+    """mc_nn, j_nn and the converging-path mc_new of nndescent.py:100-101, 107.
+
+    The reference slices ``indices[:, :mc_new]``, so at most k sources are used;
+    for k < 3 its floor of 3 sources makes its reshape fail, here it is clamped."""
+    mc_nn = max(3, int(min(k, mc) * min(1.0, update_frac ** 0.5 * 3)))
+    j_nn = max(k // 2, min(k, int(k * min(1.0, update_frac ** 0.5 * 3))))
+    mc_conv = max(3, int(k * update_frac))
+    return min(mc_nn, k), j_nn, min(mc_conv, k)
+
+
+def random_start(n: int, k: int, d: int, random_state):
+    """The reference's draws, in its order (nndescent.py:47-57, 72-82)."""
+    if random_state is not None:
+        np.random.seed(random_state)
+    idx = np.random.randint(0, n - 1, (n, k), dtype=np.int32)
+    i_vals = np.arange(n, dtype=np.int32)[:, None]
+    idx = np.where(idx >= i_vals, idx + 1, idx).astype(np.int32)
+    pd1, pd2 = min(100, d), min(300, d)
+    P = (np.random.randn(d, pd1).astype(np.float32) / np.sqrt(pd1)).astype(np.float32) if pd1 < d else None
+    P2 = (np.random.randn(d, pd2).astype(np.float32) / np.sqrt(pd2)).astype(np.float32) if pd2 < d else None
+    return idx, P, P2
 
 
 class NNDescent:
@@ -20,11 +69,132 @@ class NNDescent:
         self.random_state = random_state
         self.verbose = verbose
         self.neighbor_graph = None
+        self.history_ = []
 
     def build(self, X) -> tuple[np.ndarray, np.ndarray]:
+        """Returns (indices int32 (n, k), Euclidean distances float32 (n, k)) on the host."""
         idx, dist = self.build_device(to_device_f32(X))
         self.neighbor_graph = (to_host(idx).astype(np.int32), to_host(dist).astype(np.float32))
         return self.neighbor_graph
 
+    # ------------------------------------------------------------------
     def build_device(self, X: torch.Tensor):
-        raise NotImplementedError("NNDescent kernels are not built yet")
+        """Device version of build: (idx int32, Euclidean dist float32) CUDA tensors."""
+        if not isinstance(X, torch.Tensor) or not X.is_cuda:
+            X = to_device_f32(X)
+        X = X.contiguous().float()
+        n, d = X.shape
+        if n < 2:
+            raise ValueError("NNDescent needs at least 2 points")
+        k = min(self.k, n - 1)
+        if k > 32:
+            raise ValueError("NNDescent on the GPU supports k <= 32")
+        mc = self.max_candidates or k
+        dev = X.device
+        _lib.load()
+        s = stream_handle()
+
+        idx_h, P, P2 = random_start(n, k, d, self.random_state)
+        idx = torch.from_numpy(idx_h).to(dev, non_blocking=True)
+        dist = torch.empty((n, k), dtype=torch.float32, device=dev)
+        sq = torch.empty(n, dtype=torch.float32, device=dev)
+        call("umapb_nnd_sqnorms", ptr(X), n, d, 0, ptr(sq), s)
+        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
+
+        if P is not None:
+            with _no_tf32():
+                X_low = (X @ torch.from_numpy(P).to(dev)).contiguous()
+            sq_low = torch.empty(n, dtype=torch.float32, device=dev)
+            call("umapb_nnd_sqnorms", ptr(X_low), n, X_low.shape[1], 0, ptr(sq_low), s)
+        else:
+            X_low, sq_low = X, sq
+        P2_d = torch.from_numpy(P2).to(dev) if P2 is not None else None
+
+        rev = torch.empty((n, k), dtype=torch.int32, device=dev)
+        rev_ws = _lib.workspace(query("umapb_nnd_reverse_workspace", n, k), dev)
+        idx2 = torch.empty_like(idx)
+        dist2 = torch.empty_like(dist)
+        flags = torch.ones((n, k), dtype=torch.uint8, device=dev)
+        flags2 = torch.empty_like(flags)
+        changed = torch.zeros(1, dtype=torch.int64, device=dev)
+        Xh = None
+
+        t0 = time.time()
+        update_frac = 1.0
+        self.history_ = []
+        for it in range(self.n_iters):
+            mc_nn, j_nn, mc_conv = iteration_params(update_frac, k, mc)
+            use_rev = update_frac >= 0.10
+            if use_rev:
+                call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
+            changed.zero_()
+            if update_frac < 0.5:
+                # converging path: FP32, full dimension, stored distances
+                call("umapb_nnd_iteration", ptr(X), ptr(sq), d, 0, ptr(idx), ptr(dist), ptr(flags),
+                     ptr(rev if use_rev else None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2),
+                     ptr(changed), s)
+                info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev)
+            else:
+                if it == 0:
+                    Xd, sqd = X_low, sq_low
+                elif it == 1 and P2_d is not None:
+                    with _no_tf32():
+                        Xd = (X @ P2_d).contiguous()
+                    sqd = torch.empty(n, dtype=torch.float32, device=dev)
+                    call("umapb_nnd_sqnorms", ptr(Xd), n, Xd.shape[1], 0, ptr(sqd), s)
+                else:
+                    Xd, sqd = X, sq
+                use_half = it in (1, 2, 3, 4)
+                recompute = (it == 0) or use_half
+                dd = Xd.shape[1]
+                if use_half:
+                    if Xd is X:
+                        if Xh is None:
+                            Xh = torch.empty((n, d), dtype=torch.float16, device=dev)
+                            call("umapb_nnd_to_half", ptr(X), n * d, ptr(Xh), s)
+                        src = Xh
+                    else:
+                        src = torch.empty((n, dd), dtype=torch.float16, device=dev)
+                        call("umapb_nnd_to_half", ptr(Xd), n * dd, ptr(src), s)
+                else:
+                    src = Xd
+                call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, int(use_half), ptr(idx), ptr(dist), ptr(None),
+                     ptr(rev if use_rev else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2), ptr(dist2),
+                     ptr(flags2), ptr(changed), s)
+                if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)
+                    call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx2), ptr(dist2), k, 0, s)
+                info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd)
+            n_changed = int(changed.item())  # the one host read per iteration
+            update_frac = n_changed / (n * k)
+            idx, idx2 = idx2, idx
+            dist, dist2 = dist2, dist
+            flags, flags2 = flags2, flags
+            info.update(it=it, changed=n_changed)
+            self.history_.append(info)
+            if self.verbose:
+                print(f"Iter {it + 1}/{self.n_iters}: {n_changed} updates ({update_frac:.4f}), "
+                      f"{time.time() - t0:.2f}s")
+            if update_frac < self.delta:
+                if self.verbose:
+                    print(f"Converged at iteration {it + 1}")
+                break
+        out = torch.empty_like(dist)
+        _sqrt_into(dist, out)
+        return idx, out
+
+
+class _no_tf32:
+    """Keeps the projection GEMMs in full FP32, like the reference's X @ P."""
+
+    def __enter__(self):
+        self.prev = torch.backends.cuda.matmul.allow_tf32
+        torch.backends.cuda.matmul.allow_tf32 = False
+
+    def __exit__(self, *exc):
+        torch.backends.cuda.matmul.allow_tf32 = self.prev
+
+
+def _sqrt_into(d2: torch.Tensor, out: torch.Tensor) -> None:
+    """Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400) with the library kernel."""
+    call("umapb_nnd_sqrt", ptr(d2), d2.numel(), ptr(out), stream_handle())
+

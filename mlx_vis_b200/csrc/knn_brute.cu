@@ -153,8 +153,11 @@ __device__ __forceinline__ bool key_lt2(float a, int ia, float b, int ib) {
   return a < b || (a == b && ia < ib);
 }
 
+// Compare-exchange on the score alone: which of two equal scores survives at the
+// 32nd slot does not change the result, because the exact rerank orders the
+// surviving candidates by (distance, index).
 __device__ __forceinline__ void cex(float& a, int& ia, float& b, int& ib, bool ascending) {
-  const bool sw = ascending ? key_lt2(b, ib, a, ia) : key_lt2(a, ia, b, ib);
+  const bool sw = ascending ? (b < a) : (a < b);
   const float ta = a, tb = b;
   const int xa = ia, xb = ib;
   a = sw ? tb : ta;
@@ -187,7 +190,7 @@ __device__ __forceinline__ void merge_32_16(float (&lv)[32], int (&li)[32], cons
   for (int i = 16; i < 32; ++i) {
     const float b = bv[31 - i];
     const int ib = bx[31 - i];
-    if (key_lt2(b, ib, lv[i], li[i])) {
+    if (b < lv[i]) {
       lv[i] = b;
       li[i] = ib;
     }

@@ -202,41 +202,38 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
   if (j >= n) return;
   const int cnt = deg[j];
   const int32_t* b = bucket + off[j];
-  // k passes: each finds the smallest source above the previous pick (sources are distinct
-  // except when a row lists j twice; then it is repeated, like the reference's sort keeps it)
-  int prev = -1, prev_mult = 0;
+  // The sorted multiset of j's sources, first k of it: each pass emits the previous
+  // source again while it has unused copies (a row that lists j twice), else the
+  // next larger source; once the bucket is exhausted the remaining slots stay 0,
+  // as the reference's scatter into zeros leaves them.
+  int prev = -1, used = 0, copies = 0;
   for (int p = 0; p < k; ++p) {
-    int best = 0x7fffffff;
-    int mult = 0;
-    for (int t = lane; t < cnt; t += 32) {
-      const int s = b[t];
-      if (s > prev && s < best) best = s;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
-    // multiplicity of prev: emit prev again while it has unused copies
-    int cprev = 0;
-    if (prev >= 0) {
-      for (int t = lane; t < cnt; t += 32) cprev += b[t] == prev ? 1 : 0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) cprev += __shfl_xor_sync(0xffffffffu, cprev, o);
-    }
     int out;
-    if (prev >= 0 && prev_mult < cprev) {
+    if (prev >= 0 && used < copies) {
       out = prev;
-      mult = prev_mult + 1;
-    } else if (best != 0x7fffffff) {
-      out = best;
-      mult = 1;
+      ++used;
     } else {
-      out = 0;  // empty slot: zero, as the reference's scatter into zeros leaves it
-      mult = prev_mult;
+      int best = 0x7fffffff;
+      for (int t = lane; t < cnt; t += 32) {
+        const int s = b[t];
+        if (s > prev && s < best) best = s;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+      if (best == 0x7fffffff) {
+        for (int q = p + lane; q < k; q += 32) rev[j * k + q] = 0;
+        return;
+      }
+      int c = 0;
+      for (int t = lane; t < cnt; t += 32) c += b[t] == best ? 1 : 0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      out = best;
+      prev = best;
+      copies = c;
+      used = 1;
     }
     if (lane == 0) rev[j * k + p] = out;
-    if (out != 0 || best != 0x7fffffff) {
-      if (out != prev) prev = out;
-      prev_mult = mult;
-    }
   }
 }
 
@@ -365,9 +362,15 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
     dot4<T>(reinterpret_cast<const T*>(a.Xd), xs, a.dd, c, cnt, lane, dots);
     if (lane < cnt) {
       float dot = dots[0];
+      int my_t = tt[0], my_c = c[0];
+#pragma unroll
       for (int u = 1; u < 4; ++u)
-        if (lane == u) dot = dots[u];
-      cd[tt[lane]] = d2_from_dot(sqi, a.sqd[c[lane]], dot, a.half_round != 0);
+        if (lane == u) {
+          dot = dots[u];
+          my_t = tt[u];
+          my_c = c[u];
+        }
+      cd[my_t] = d2_from_dot(sqi, a.sqd[my_c], dot, a.half_round != 0);
     }
   }
   __syncwarp();
@@ -411,6 +414,26 @@ using namespace umapb;
 static size_t iter_smem_per_warp(int dd, int elem, int tcap, int hcap) {
   const size_t per_warp = (size_t)dd * elem + (size_t)tcap * 12 + (size_t)hcap * 4 + 32 * 4 + 16;
   return (per_warp + 15) / 16 * 16;
+}
+
+namespace umapb {
+namespace nnd {
+__global__ void sqrt_kernel(const float* __restrict__ d2, int64_t m, float* __restrict__ out) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    out[t] = sqrtf(fmaxf(d2[t], 0.0f));
+}
+}  // namespace nnd
+}  // namespace umapb
+
+extern "C" int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(d2 && out && count >= 0, "nnd_sqrt: bad arguments");
+  if (count == 0) return UMAPB_OK;
+  const int64_t want = ceil_div(count, 256);
+  const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
+  nnd::sqrt_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(d2, count, out);
+  UMAPB_LAUNCH_CHECK("nnd_sqrt kernel");
+  return UMAPB_OK;
 }
 
 extern "C" int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq,

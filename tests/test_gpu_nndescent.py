@@ -1,0 +1,97 @@
+"""NNDescent on the GPU against the NumPy oracle of the reference algorithm
+(same NumPy random start and projections) and the reference's golden graphs.
+
+The GPU and the oracle make the same choices except where float rounding orders
+two nearly equal distances differently (GPU dot products are summed in another
+order, FP16 iterations round those sums), so graphs agree row-set-wise to
+within a fraction of a percent and the per-iteration change counts track."""
+
+import numpy as np
+import pytest
+
+from oracle import knn as oknn
+from oracle import nndescent as onnd
+
+pytestmark = pytest.mark.gpu
+
+
+def recall(idx, ref_idx):
+    return float(np.mean([len(set(a) & set(b)) / len(a) for a, b in zip(idx, ref_idx)]))
+
+
+@pytest.mark.parametrize("name,gen", [("nnd_gauss", ("gaussian_mixture", 3000, 32, 2)),
+                                      ("nnd_proto", ("prototype_mixture", 2000, 784, 3))])
+def test_nndescent_tracks_oracle_and_reference(name, gen, golden):
+    from mlx_vis_b200 import NNDescent, datasets
+
+    X = getattr(datasets, gen[0])(gen[1], gen[2], seed=gen[3])
+    g = golden(name)
+    its = sorted(int(k[6:]) for k in g if k.startswith("idx_it"))
+    for t in its:
+        nn = NNDescent(k=15, random_state=42, n_iters=t)
+        idx, dist = nn.build(X)
+        (oi, od), olog = onnd.build(X, k=15, random_state=42, n_iters=t, history=True)
+        agree = recall(idx, oi)
+        assert agree > 0.99, (t, agree)
+        ours = [h["changed"] for h in nn.history_]
+        theirs = [l["changed"] for l in olog]
+        assert len(ours) == len(theirs), (ours, theirs)
+        np.testing.assert_allclose(ours, theirs, rtol=0.02, atol=20)
+        gi = g[f"idx_it{t}"].astype(np.int32)
+        assert recall(idx, gi) > 0.98
+        # distances: the space of the iteration that produced them (the 100-d
+        # projection after iteration 1, FP16-rounded dots in iterations 2-5, FP32
+        # afterwards), as in the reference; compare where the lists agree
+        same = idx == oi
+        if t < 5:  # FP16 iterations: the FP16-rounded dot may differ by one FP16 ulp
+            sq = float(np.max(np.sum(X.astype(np.float64) ** 2, axis=1)))
+            ulp = 2.0 ** (np.floor(np.log2(sq)) - 10)
+            d2_err = np.abs(dist[same] ** 2 - od[same] ** 2)
+            assert np.all(d2_err <= 2.5 * ulp + 1e-3 * od[same] ** 2), d2_err.max()
+        else:  # FP32 after the recompute; a converging 5th iteration keeps FP16-era values, as the reference does
+            np.testing.assert_allclose(dist[same], od[same], rtol=1e-4, atol=1e-4)
+    # final quality equals the reference's
+    ri, _ = oknn.knn_exact_f64(X, 15)
+    assert abs(recall(idx, ri) - recall(g[f"idx_it{its[-1]}"].astype(np.int32), ri)) < 0.01
+
+
+def test_nndescent_reverse_candidates_match_oracle():
+    import torch
+
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(0)
+    n, k = 500, 15
+    idx = rng.integers(0, n, size=(n, k)).astype(np.int32)  # duplicates within rows on purpose
+    want = onnd.reverse_candidates(idx)
+    d_idx = torch.from_numpy(idx).cuda()
+    rev = torch.empty_like(d_idx)
+    ws = _lib.workspace(_lib.query("umapb_nnd_reverse_workspace", n, k), d_idx.device)
+    _lib.call("umapb_nnd_reverse", _lib.ptr(d_idx), n, k, _lib.ptr(rev), _lib.ptr(ws), ws.numel(),
+              _lib.stream_handle())
+    assert np.array_equal(rev.cpu().numpy(), want)
+
+
+def test_nndescent_small_and_edge_cases():
+    from mlx_vis_b200 import NNDescent
+
+    rng = np.random.default_rng(3)
+    for n, d, k in [(2, 3, 15), (17, 5, 15), (200, 130, 10), (1000, 100, 15)]:
+        X = rng.normal(size=(n, d)).astype(np.float32)
+        idx, dist = NNDescent(k=k, random_state=0).build(X)
+        kk = min(k, n - 1)
+        assert idx.shape == (n, kk) and dist.shape == (n, kk)
+        assert np.all(idx != np.arange(n)[:, None])
+        assert np.all(np.isfinite(dist)) and np.all(np.diff(dist, axis=1) >= -1e-3)
+        if n <= 200:
+            ri, _ = oknn.knn_exact_f64(X, kk)
+            assert recall(idx, ri) > 0.9
+
+
+def test_umap_with_nndescent(gauss2000):
+    from sklearn.manifold import trustworthiness
+
+    from mlx_vis_b200 import UMAP
+
+    Y = UMAP(n_epochs=200, knn_method="nndescent", random_state=0).fit_transform(gauss2000)
+    assert trustworthiness(gauss2000, Y, n_neighbors=15) > 0.95
