@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""UMAP fit benchmark on B200: the 70,000 x 784 full pipeline.
+
+Workload (one step = one complete fit): seeded prototype mixture 70,000 x 784
+(10 classes of 7,000; stands in for Fashion-MNIST, which is not available
+offline), NNDescent k=15 with the reference's defaults (n_iters 20, delta
+0.015), fuzzy simplicial set, spectral init, 500 layout epochs, 2 components.
+
+  value   positive-edge updates of the whole fit per second, summed over ranks
+          (edges/s of the whole fit_transform, inputs resident on the device)
+  fit_s   seconds per fit (the other half of the metric)
+  e2e     the same metric through UMAP.fit_transform on a pinned host tensor,
+          host->device input and device->host embedding copies inside the timing
+  roofline  NNDescent iteration kernel (the largest share of a fit), CUDA events
+          around each launch in the timed fits; algorithmic bytes = distance
+          evaluations x row bytes + own rows + candidate lists
+  cpu_baseline  the NumPy oracle of the reference algorithm on the host cores,
+          on a bounded sample of the workload, extrapolated per stage
+
+N > 1 (torchrun): every rank fits its own replica (weak scaling, no
+collective on the data path); time = max over ranks.
+`--impl reference` times the reference algorithm's CPU port the same way.
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "UMAP fit s & edges/s @70K×784"
+N_FULL, D, K_NN, N_EPOCHS = 70000, 784, 15, 500
+CPU_SAMPLE_N = 2000
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_FULL, help="rows (default: the 70K workload)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_data(n):
+    from mlx_vis_b200.datasets import prototype_mixture
+
+    return prototype_mixture(n, D, seed=0)
+
+
+def config(n):
+    return {"workload": f"UMAP fit_transform of a {n}x{D} seeded prototype mixture (10 classes); NNDescent k={K_NN} "
+                        f"(n_iters 20, delta 0.015), fuzzy set, spectral init, {N_EPOCHS} epochs, 2 components",
+            "n": n, "d": D, "n_neighbors": K_NN, "n_epochs": N_EPOCHS, "min_dist": 0.1, "knn_method": "nndescent",
+            "init": "spectral", "parallelism": "replicas (one independent fit per GPU)",
+            "l2": f"inputs larger than L2: X is {n * D * 4 / 1e6:.1f} MB fp32 per step"}
+
+
+# --------------------------------------------------------------------------
+def schedule_edge_updates(vals: np.ndarray, n_epochs: int) -> int:
+    """Positive-edge updates of a fit: the float32 schedule of umap.py:398-414."""
+    w = vals.astype(np.float32)
+    n_samples = n_epochs * (w / float(w.max()))
+    eps = np.where(n_samples > 0, n_epochs / n_samples, -1.0).astype(np.float32)
+    nxt = eps.copy()
+    total = 0
+    for e in range(n_epochs):
+        act = nxt <= e
+        c = int(act.sum())
+        if c:
+            nxt[act] += eps[act]
+            total += c
+    return total
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait(timeout=10)
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax.append(float(parts[2].split()[0]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the roofline kernel from the committed ncu summary, if any."""
+    path = os.path.join(HERE, "profiles", "nnd_iteration_70k.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from mlx_vis_b200 import UMAP, _lib
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+    n = args.n
+    X = make_data(n)
+    Xd = torch.from_numpy(X).cuda()
+    X_pinned = torch.from_numpy(X).pin_memory()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def make():
+        return UMAP(n_components=2, n_neighbors=K_NN, min_dist=0.1, n_epochs=N_EPOCHS, knn_method="nndescent",
+                    random_state=0)
+
+    for _ in range(max(args.warmup, 3)):
+        make().fit_transform_device(Xd)
+    u = make()
+    u.fit_transform(X_pinned)  # warm the host path too
+
+    # positive-edge updates per fit: deterministic given the graph, counted untimed
+    # from the same graph stage (NNDescent seed 0, fuzzy set) on the host
+    from mlx_vis_b200._nndescent.nndescent import NNDescent
+
+    idx, dd = NNDescent(k=K_NN, random_state=0).build_device(Xd)
+    rows, cols, vals, ne = _lib.fuzzy(idx, dd, N_EPOCHS, fp64=True)
+    E = int(ne.item())
+    edges_per_fit = schedule_edge_updates(vals[:E].cpu().numpy(), N_EPOCHS)
+
+    # ---- device-resident timing ----
+    launches0 = _lib.kernel_launches()
+    models = [make() for _ in range(args.steps)]
+    for m in models:
+        m.profile_kernels = True
+    barrier()
+    clk = Clocks(local_rank)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for m in models:
+        m.fit_transform_device(Xd)
+    t1.record()
+    barrier()
+    clocks = clk.stop()
+    launches = _lib.kernel_launches() - launches0
+    ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+
+    # roofline of the NNDescent iteration kernel from the events of the timed fits
+    durs, bytes_ = [], []
+    for m in models:
+        for e0, e1, info in m.nndescent_.kernel_log_:
+            durs.append(e0.elapsed_time(e1) * 1e-3)
+            s, dsp, kk, T = info["elem"], info["space"], info["k"], info["candidates"]
+            bytes_.append((info["evals"] + info["n"]) * dsp * s + info["n"] * (kk + T) * 8)
+    avg_t = sum(durs) / len(durs)
+    avg_b = sum(bytes_) / len(bytes_)
+    peak, peak_kind = measured_peaks()
+    achieved = avg_b / avg_t / 1e9
+    roofline = {"kernel": "nndescent iter_kernel", "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 3),
+                "traffic": committed_traffic(), "algorithmic_bytes_per_launch": int(avg_b),
+                "avg_launch_ms": round(avg_t * 1e3, 3), "launches_per_fit": len(durs) // args.steps}
+
+    # ---- end to end through the public API (pinned host input, host output) ----
+    barrier()
+    h0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        Y = make().fit_transform(X_pinned)
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    e2e_wall = (time.perf_counter() - h0) * 1e3 / args.steps
+    if dist is not None:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    iters = len(models[-1].nndescent_.history_)
+    h2d = n * D * 4 + n * K_NN * 4 + D * 100 * 4 + D * 300 * 4 + n * 2 * 4
+    d2h = n * 2 * 4 + iters * 16
+
+    out = None
+    if rank == 0:
+        stages = models[-1].timings_
+        out = {"metric": METRIC, "value": edges_per_fit * world / (ms * 1e-3), "unit": "edges/s",
+               "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 3),
+               "fit_s": round(ms * 1e-3, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "fp32 (fp16 NNDescent iterations 1-4 and bf16 brute-force tiles as in the design; fp64 sigma)",
+               "data": "synthetic (seeded prototype mixture standing in for Fashion-MNIST)",
+               "config": config(n),
+               "edges_per_fit": edges_per_fit, "n_edges_graph": E,
+               "stage_ms": {k: round(v, 2) for k, v in stages.items()},
+               "layout_edges_per_s": edges_per_fit / (stages["layout"] * 1e-3),
+               "roofline": roofline,
+               "e2e": {"value": edges_per_fit * world / (e2e_ms * 1e-3), "unit": "edges/s", "fit_s": round(e2e_ms * 1e-3, 4),
+                       "wall_ms_per_step": round(e2e_wall, 2), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+               "gpu_launches": launches, "gpu_launches_per_step": launches // args.steps,
+               "clocks": clocks}
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_baseline():
+    from oracle.pipeline import estimate_fit
+
+    r = estimate_fit(N_FULL, make_data, CPU_SAMPLE_N, n_epochs=N_EPOCHS, k=K_NN)
+    return {"value": r["edge_updates_full"] / r["fit_s_full"], "unit": "edges/s", "fit_s": round(r["fit_s_full"], 2),
+            "cores": r["threads"], "kind": "port",
+            "sample": r["sample"] + f"; extrapolated to {N_FULL} rows per stage (NNDescent, fuzzy set and spectral "
+                                    "init by rows, layout by positive-edge updates)",
+            "stage_s": {k: round(v, 2) for k, v in r["stage_s_full"].items()}, "cpu_s": round(r["cpu_s"], 2)}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    for _ in range(max(args.warmup, 3)):
+        cpu_baseline()
+    vals, fits = [], []
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        cb = cpu_baseline()
+        vals.append(cb["value"])
+        fits.append(cb["fit_s"])
+    ms = (time.perf_counter() - t) * 1e3 / args.steps
+    v = statistics.mean(vals)
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 1), "fit_s": round(statistics.mean(fits), 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic (seeded prototype mixture standing in for Fashion-MNIST)", "config": config(N_FULL),
+            "cpu_baseline": {"value": v, "unit": "edges/s", "kind": "port", "cores": cb["cores"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+    if out is not None and rank == 0:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

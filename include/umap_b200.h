@@ -41,6 +41,9 @@ typedef struct CUstream_st* umapb_stream_t;
 const char* umapb_last_error(void);
 /* ABI version of this library. */
 int umapb_abi_version(void);
+/* Number of CUDA kernels this library has enqueued in this process so far
+ * (kernels recorded into a CUDA graph count once, at capture). */
+unsigned long long umapb_kernel_launches(void);
 /* Synchronises `stream`, reads the device status word at `workspace` and
  * returns UMAPB_OK or UMAPB_ERR_DEVICE (with a message). */
 int umapb_read_status(const void* workspace, umapb_stream_t stream);
@@ -80,7 +83,8 @@ int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t ext
  *                     when half != 0), stored distances reused for current
  *                     neighbours unless recompute_cur, self and duplicates 1e30,
  *                     the k smallest (distance, id) kept; flags_new = positional
- *                     change flags, *changed (device uint64) += their count.
+ *                     change flags, *changed (device uint64) += their count,
+ *                     *evals (device uint64, nullable) += distances evaluated.
  *                     Rows without a NEW flag are copied on the converging path.
  * umapb_nnd_sqrt:     Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400).
  * ------------------------------------------------------------------------- */
@@ -94,7 +98,8 @@ int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, vo
 int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t half, const int32_t* idx_old,
                         const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n, int32_t k,
                         int32_t mc_new, int32_t j_nn, int32_t converging, int32_t recompute_cur, int32_t* idx_new,
-                        float* dist_new, uint8_t* flags_new, unsigned long long* changed, umapb_stream_t stream);
+                        float* dist_new, uint8_t* flags_new, unsigned long long* changed,
+                        unsigned long long* evals, umapb_stream_t stream);
 int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------

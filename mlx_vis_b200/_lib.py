@@ -44,13 +44,19 @@ SIGNATURES = {
     "umapb_nnd_reverse_workspace": [_i64, _i32, _psz],
     "umapb_nnd_reverse": [_p, _i64, _i32, _p, _p, _sz, _p],
     "umapb_nnd_iteration": [_p, _p, _i32, _i32, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _i32, _i32, _p, _p, _p, _p,
-                            _p],
+                            _p, _p],
+    "umapb_kernel_launches": [],
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],
 }
-_RESTYPES = {"umapb_last_error": _c.c_char_p}
+_RESTYPES = {"umapb_last_error": _c.c_char_p, "umapb_kernel_launches": _c.c_ulonglong}
+
+
+def kernel_launches() -> int:
+    """Kernels this library has enqueued in this process (graph captures count once)."""
+    return int(load().umapb_kernel_launches())
 
 _lock = threading.Lock()
 _lib = None

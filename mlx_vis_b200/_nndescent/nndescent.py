@@ -70,6 +70,12 @@ class NNDescent:
         self.verbose = verbose
         self.neighbor_graph = None
         self.history_ = []
+        self.profile_kernels = False  # record CUDA events around each iteration kernel
+
+    def _events(self):
+        if not self.profile_kernels:
+            return None
+        return (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
 
     def build(self, X) -> tuple[np.ndarray, np.ndarray]:
         """Returns (indices int32 (n, k), Euclidean distances float32 (n, k)) on the host."""
@@ -117,7 +123,9 @@ class NNDescent:
         flags = torch.ones((n, k), dtype=torch.uint8, device=dev)
         flags2 = torch.empty_like(flags)
         changed = torch.zeros(1, dtype=torch.int64, device=dev)
+        evals = torch.zeros(1, dtype=torch.int64, device=dev)
         Xh = None
+        self.kernel_log_ = []  # (start event, end event, info) per iteration kernel when profile_kernels
 
         t0 = time.time()
         update_frac = 1.0
@@ -128,12 +136,16 @@ class NNDescent:
             if use_rev:
                 call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
             changed.zero_()
+            evals.zero_()
+            ev = self._events()
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
+                ev[0].record() if ev else None
                 call("umapb_nnd_iteration", ptr(X), ptr(sq), d, 0, ptr(idx), ptr(dist), ptr(flags),
                      ptr(rev if use_rev else None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2),
-                     ptr(changed), s)
-                info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev)
+                     ptr(changed), ptr(evals), s)
+                ev[1].record() if ev else None
+                info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4)
             else:
                 if it == 0:
                     Xd, sqd = X_low, sq_low
@@ -158,18 +170,24 @@ class NNDescent:
                         call("umapb_nnd_to_half", ptr(Xd), n * dd, ptr(src), s)
                 else:
                     src = Xd
+                ev[0].record() if ev else None
                 call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, int(use_half), ptr(idx), ptr(dist), ptr(None),
                      ptr(rev if use_rev else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2), ptr(dist2),
-                     ptr(flags2), ptr(changed), s)
+                     ptr(flags2), ptr(changed), ptr(evals), s)
+                ev[1].record() if ev else None
                 if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)
                     call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx2), ptr(dist2), k, 0, s)
-                info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd)
+                info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd,
+                            elem=2 if use_half else 4)
             n_changed = int(changed.item())  # the one host read per iteration
             update_frac = n_changed / (n * k)
             idx, idx2 = idx2, idx
             dist, dist2 = dist2, dist
             flags, flags2 = flags2, flags
-            info.update(it=it, changed=n_changed)
+            info.update(it=it, changed=n_changed, evals=int(evals.item()), n=n, k=k,
+                        candidates=k + info["mc_new"] * j_nn + (k if use_rev else 0))
+            if ev:
+                self.kernel_log_.append((ev[0], ev[1], info))
             self.history_.append(info)
             if self.verbose:
                 print(f"Iter {it + 1}/{self.n_iters}: {n_changed} updates ({update_frac:.4f}), "

@@ -84,6 +84,7 @@ class UMAP:
         self.embedding_ = None
         self.timings_ = {}
         self.graph_ = None
+        self.profile_kernels = False  # CUDA events around NNDescent iteration kernels (bench roofline)
 
     # ------------------------------------------------------------------
     def fit_transform(self, X, epoch_callback=None) -> np.ndarray:
@@ -113,11 +114,19 @@ class UMAP:
 
         if self.verbose:
             print("Computing nearest neighbors...")
-        from mlx_vis_b200._knn import knn_device
+        from mlx_vis_b200._knn import RERANK_EXTRA, resolve_method
+        from mlx_vis_b200._nndescent.nndescent import NNDescent
 
         k = min(self.n_neighbors, n - 1)
-        knn_idx, knn_dist = knn_device(Xd, k, method=self.knn_method, verbose=self.verbose,
-                                       random_state=self.random_state)
+        if resolve_method(self.knn_method, n) == "nndescent":  # _knn.py:35-45
+            nn = NNDescent(k=k, verbose=self.verbose,
+                           random_state=self.random_state if self.random_state is not None else 42)
+            nn.profile_kernels = self.profile_kernels
+            knn_idx, knn_dist = nn.build_device(Xd)
+            self.nndescent_ = nn
+        else:
+            knn_idx, knn_dist = _lib.knn_brute(Xd, k, extra=RERANK_EXTRA)
+            self.nndescent_ = None
         ev.mark("knn")
 
         if self.n_epochs is None:

@@ -6,6 +6,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -30,6 +31,10 @@ int check_cuda(const char* what) {
   if (e != cudaSuccess) return set_error(UMAPB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return UMAPB_OK;
 }
+
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launches(int k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
 
 int num_sms() {
   int dev = 0;
@@ -82,6 +87,8 @@ extern "C" {
 const char* umapb_last_error(void) { return umapb::g_msg; }
 
 int umapb_abi_version(void) { return 1; }
+
+unsigned long long umapb_kernel_launches(void) { return umapb::g_launches.load(std::memory_order_relaxed); }
 
 int umapb_read_status(const void* workspace, umapb_stream_t stream) {
   umapb::clear_error();

@@ -18,6 +18,10 @@ void clear_error();
 // Converts the last CUDA runtime error (if any) into a status.
 int check_cuda(const char* what);
 
+// Adds to the process-wide count of kernels this library has enqueued
+// (reported by umapb_kernel_launches()).
+void count_launches(int k);
+
 #define UMAPB_REQUIRE(cond, ...)                                          \
   do {                                                                    \
     if (!(cond)) return ::umapb::set_error(UMAPB_ERR_ARG, __VA_ARGS__);   \

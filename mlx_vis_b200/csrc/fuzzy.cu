@@ -237,5 +237,6 @@ extern "C" int umapb_fuzzy(const int32_t* knn_idx, const float* knn_dist, int64_
   fuzzy::prune_write_kernel<<<(unsigned)nb, fuzzy::kBlock, 0, stream>>>(l.w_sym, knn_idx, m, k, l.wmax, n_epochs,
                                                                        l.block_counts, rows, cols, vals);
   UMAPB_LAUNCH_CHECK("fuzzy: prune write kernel");
+  count_launches(5);
   return UMAPB_OK;
 }

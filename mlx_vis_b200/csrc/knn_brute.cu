@@ -742,5 +742,6 @@ extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, 
                                                                       p.L, P, PL, k, squared, out_idx, out_dist);
     UMAPB_LAUNCH_CHECK("knn_brute: rerank kernel launch");
   }
+  count_launches(3);
   return UMAPB_OK;
 }

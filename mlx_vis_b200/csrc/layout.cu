@@ -349,6 +349,7 @@ extern "C" int umapb_layout_prepare(const float* vals, const int64_t* n_edges, i
   layout::max_kernel<<<g, layout::kBlock, 0, stream>>>(vals, n_edges, l.wmax);
   layout::eps_kernel<<<g, layout::kBlock, 0, stream>>>(vals, n_edges, l.wmax, n_epochs, eps, next);
   UMAPB_LAUNCH_CHECK("layout_prepare kernels");
+  count_launches(2);
   return UMAPB_OK;
 }
 
@@ -380,6 +381,7 @@ extern "C" int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32
     }
   }
   UMAPB_LAUNCH_CHECK("layout_epochs kernels");
+  count_launches(2 * (epoch_end - epoch_begin));
   return UMAPB_OK;
 }
 
@@ -398,6 +400,7 @@ extern "C" int umapb_layout_count_active(const float* next, const int64_t* n_edg
   layout::count_active_kernel<<<(unsigned)nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
   scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, nb, count);
   UMAPB_LAUNCH_CHECK("layout_count_active kernels");
+  count_launches(2);
   return UMAPB_OK;
 }
 
@@ -439,5 +442,6 @@ extern "C" int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, con
     default: layout::launch_injected<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch, p, neg_rate, neg_to, stream); break;
   }
   UMAPB_LAUNCH_CHECK("layout_epoch_injected kernels");
+  count_launches(4);
   return UMAPB_OK;
 }

@@ -254,6 +254,7 @@ struct IterArgs {
   float* dist_new;
   uint8_t* flags_new;
   unsigned long long* changed;
+  unsigned long long* evals;  // nullable: distance evaluations performed
 };
 
 template <class T>
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
   }
   const int nch = __popc(__ballot_sync(0xffffffffu, lane < k && li != my_old));
   if (lane == 0 && nch) atomicAdd(a.changed, (unsigned long long)nch);
+  if (lane == 0 && a.evals) atomicAdd(a.evals, (unsigned long long)n_todo);
 }
 
 }  // namespace nnd
@@ -433,6 +435,7 @@ extern "C" int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_
   const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
   nnd::sqrt_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(d2, count, out);
   UMAPB_LAUNCH_CHECK("nnd_sqrt kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
 
@@ -447,6 +450,7 @@ extern "C" int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t h
   else
     nnd::sqnorm_kernel<float><<<blocks, 256, 0, stream>>>(static_cast<const float*>(X), n, dd, sq);
   UMAPB_LAUNCH_CHECK("nnd_sqnorms kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
 
@@ -459,6 +463,7 @@ extern "C" int umapb_nnd_to_half(const float* X, int64_t count, void* H, umapb_s
   nnd::to_half_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(X, count,
                                                                                     static_cast<__half*>(H));
   UMAPB_LAUNCH_CHECK("nnd_to_half kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
 
@@ -479,6 +484,7 @@ extern "C" int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int3
   nnd::gather_rows_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, smem,
                             reinterpret_cast<cudaStream_t>(stream_)>>>(X, sq, n, dd, idx, dist, k, sort_rows);
   UMAPB_LAUNCH_CHECK("nnd_gather kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
 
@@ -524,6 +530,7 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
                                                                                                   n, k, rev);
   UMAPB_LAUNCH_CHECK("nnd_reverse kernels");
+  count_launches(4);
   return UMAPB_OK;
 }
 
@@ -531,7 +538,8 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
                                    const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n,
                                    int32_t k, int32_t mc_new, int32_t j_nn, int32_t converging,
                                    int32_t recompute_cur, int32_t* idx_new, float* dist_new, uint8_t* flags_new,
-                                   unsigned long long* changed, umapb_stream_t stream_) {
+                                   unsigned long long* changed, unsigned long long* evals,
+                                   umapb_stream_t stream_) {
   clear_error();
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(Xd && sqd && idx_old && dist_old && idx_new && dist_new && flags_new && changed,
@@ -564,6 +572,7 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.dist_new = dist_new;
   a.flags_new = flags_new;
   a.changed = changed;
+  a.evals = evals;
   const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(dd, half ? 2 : 4, a.tcap, a.hcap);
   UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_iteration: row dimension too large for shared memory");
   static bool attr = false;
@@ -582,5 +591,6 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   else
     nnd::iter_kernel<float><<<blocks, nnd::kWarps * 32, smem, stream>>>(a);
   UMAPB_LAUNCH_CHECK("nnd_iteration kernel");
+  count_launches(1);
   return UMAPB_OK;
 }

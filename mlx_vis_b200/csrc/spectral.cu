@@ -308,6 +308,7 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
                                                                      l.red + 5);
   spectral::minmax_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, n, dim, l.red + 1, l.red + 5, Y);
   UMAPB_LAUNCH_CHECK("spectral: rescale kernels");
+  count_launches((e_cap > 0 ? 3 : 2) + 1 + n_iter + 4);
   return UMAPB_OK;
 }
 
@@ -320,5 +321,6 @@ extern "C" int umapb_normal_fill(float* out, int64_t count, uint64_t seed, umapb
   spectral::normal_fill_kernel<<<(unsigned)ceil_div(blocks4, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
       out, count, (uint32_t)seed, (uint32_t)(seed >> 32));
   UMAPB_LAUNCH_CHECK("normal_fill kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
