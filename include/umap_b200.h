@@ -64,6 +64,27 @@ int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t ext
                     umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Allocation-free brute-force kNN.  No counterpart in the reference: an extra
+ * entry point for callers that cannot allocate device memory (cudaMalloc and
+ * cudaFree synchronise the device, fail when another framework's pooled
+ * allocator owns the memory, and thin FFI bindings may be unable to keep a
+ * workspace alive).  Same arguments and results as umapb_knn_brute without the
+ * workspace: the scratch is a static device array of
+ * UMAPB_NOALLOC_SCRATCH_BYTES per GPU, held from library load until exit.
+ *   - requests needing more scratch (about 3.8 KB per row at d = 784, k = 15)
+ *     fail with UMAPB_ERR_UNSUPPORTED;
+ *   - the first call on a device looks up the array's address on that device;
+ *     make it before any stream capture;
+ *   - every call reuses the same array: calls that overlap on the GPU race, so
+ *     serialise them (one stream, or wait between calls);
+ *   - device_status (device int32, may be NULL) receives the kernels'
+ *     bounded-wait status (0 = ok) once the stream reaches the end of the call.
+ * ------------------------------------------------------------------------- */
+#define UMAPB_NOALLOC_SCRATCH_BYTES (32u << 20)
+int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                            int32_t* out_idx, float* out_dist, int32_t* device_status, umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * NNDescent — replaces NNDescent.build (mlx_vis/_nndescent/nndescent.py:34-403);
  * the host keeps the reference's iteration control and random draws.  k <= 32.
  * umapb_nnd_sqnorms:  sq[i] = |X_i|^2 (X float32, or FP16 when half != 0).

@@ -29,6 +29,7 @@ SIGNATURES = {
     "umapb_read_status": [_p, _p],
     "umapb_knn_brute_workspace": [_i64, _i64, _i32, _i32, _psz],
     "umapb_knn_brute": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _sz, _p],
+    "umapb_knn_brute_noalloc": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _p],
     "umapb_fuzzy_workspace": [_i64, _i32, _psz],
     "umapb_fuzzy": [_p, _p, _i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "umapb_normal_fill": [_p, _i64, _u64, _p],

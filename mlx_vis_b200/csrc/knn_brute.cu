@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <math.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -742,6 +743,99 @@ extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, 
                                                                       p.L, P, PL, k, squared, out_idx, out_dist);
     UMAPB_LAUNCH_CHECK("knn_brute: rerank kernel launch");
   }
+  count_launches(3);
+  return UMAPB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of umapb_knn_brute.
+//
+// Some callers cannot hand this library a device workspace: cudaMalloc and
+// cudaFree synchronise the whole device (a stall that latency-bound callers
+// cannot take), they fail outright when another framework's pooled allocator
+// already owns the device memory, and thin FFI bindings often have no way to
+// keep a device buffer alive between calls.  This entry point therefore uses a
+// fixed scratch array that lives in the library itself: a file-scope
+// __device__ array of UMAPB_NOALLOC_SCRATCH_BYTES, which every GPU that loads
+// the library holds until the process exits.  Requests whose workspace would
+// exceed it are rejected.  The first call on each device looks up that
+// device's address of the array with cudaGetSymbolAddress (with the device
+// current); make that first call before any stream capture begins.  All calls
+// share the one array and it keeps the previous call's contents, so the parts
+// that must start at zero (the status word and the candidate lists) are reset
+// by each call, and calls whose work overlaps on the GPU (for example on two
+// streams at once) race on it: serialise them.
+// ---------------------------------------------------------------------------
+namespace {
+
+static __device__ __align__(256) unsigned char g_knn_scratch[UMAPB_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_scratch_mu;
+void* g_scratch_addr[64] = {nullptr};
+
+int scratch_address(void** out) {
+  int dev = 0;
+  UMAPB_CUDA_TRY(cudaGetDevice(&dev), "knn_brute_noalloc: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute_noalloc: device index %d", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_knn_scratch);
+    if (e != cudaSuccess)
+      return set_error(UMAPB_ERR_CUDA, "knn_brute_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return UMAPB_OK;
+}
+
+}  // namespace
+
+extern "C" int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra,
+                                       int32_t squared, int32_t* out_idx, float* out_dist, int32_t* device_status,
+                                       umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(X && out_idx && out_dist, "knn_brute_noalloc: null array argument");
+  knn::Plan p;
+  int s = knn::make_plan(n, d, k, extra, nullptr, p);
+  if (s) return s;
+  if (p.ws_bytes > (size_t)UMAPB_NOALLOC_SCRATCH_BYTES)
+    return set_error(UMAPB_ERR_UNSUPPORTED,
+                     "knn_brute_noalloc: n=%lld, d=%lld, k+extra=%d needs %zu bytes of scratch but the static array "
+                     "holds %zu; use umapb_knn_brute with a caller-owned workspace",
+                     (long long)n, (long long)d, p.L, p.ws_bytes, (size_t)UMAPB_NOALLOC_SCRATCH_BYTES);
+  void* scratch = nullptr;
+  if ((s = scratch_address(&scratch))) return s;
+  knn::make_plan(n, d, k, extra, scratch, p);
+
+  UMAPB_CUDA_TRY(cudaMemsetAsync(p.status, 0, sizeof(int32_t), stream), "knn_brute_noalloc: status reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(p.cand_i, 0xFF, (size_t)n * p.slots * p.L * sizeof(int32_t), stream),
+                 "knn_brute_noalloc: candidate reset");
+  knn::prep_kernel<<<(unsigned)ceil_div(n * 32, 256), 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
+  UMAPB_LAUNCH_CHECK("knn_brute_noalloc: prep kernel launch");
+  CUtensorMap ta, tb;
+  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BM, knn::BK))) return s;
+  if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BN, knn::BK))) return s;
+  if (p.lcap == 32)
+    s = knn::launch_topk<32>(p, ta, tb, stream);
+  else if (p.lcap == 64)
+    s = knn::launch_topk<64>(p, ta, tb, stream);
+  else
+    s = knn::launch_topk<128>(p, ta, tb, stream);
+  if (s) return s;
+  const int P = knn::next_pow2(p.slots * p.L);
+  const int PL = knn::next_pow2(p.L);
+  const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);
+  if (smem > 48 * 1024)
+    return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute_noalloc: candidate merge needs %zu bytes of shared memory",
+                     smem);
+  knn::rerank_kernel<<<(unsigned)ceil_div(n, knn::RR_WARPS), knn::RR_WARPS * 32, smem, stream>>>(
+      X, n, (int)d, p.cand_s, p.cand_i, p.slots, p.L, P, PL, k, squared, out_idx, out_dist);
+  UMAPB_LAUNCH_CHECK("knn_brute_noalloc: rerank kernel launch");
+  if (device_status)
+    UMAPB_CUDA_TRY(cudaMemcpyAsync(device_status, p.status, sizeof(int32_t), cudaMemcpyDeviceToDevice, stream),
+                   "knn_brute_noalloc: status copy");
   count_launches(3);
   return UMAPB_OK;
 }
