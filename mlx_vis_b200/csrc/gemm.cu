@@ -1,0 +1,221 @@
+// BF16 tensor-core GEMM with fused MLP epilogues, for the learned warm-start
+// encoder (no counterpart in the reference; its nearest idiom is the MMAE MLP,
+// mlx_vis/_mmae/mmae.py:22-38, 258-281).
+//
+//   C[M, N] = sum_k A[m, k] B[n, k]      A (M x K), B (N x K): BF16, K-major
+//
+// One CTA per 128 x 128 output tile: warp 0 streams 64-wide K blocks of A and B
+// with TMA (128-byte swizzle, zero fill past M, N, K) through 4 stages, one thread
+// of warp 1 issues tcgen05.mma (M=128, N=128, K=16, FP32 accumulation in TMEM),
+// warps 2-5 (one per TMEM lane quarter) read the accumulator with tcgen05.ld and
+// apply the epilogue:
+//   EPI_F32        C (f32, row-major, pitch ldc)
+//   EPI_BIAS_GELU  z = C + bias[n]; Z (f32), H = bf16(gelu(z)) row-major and,
+//                  when HT != null, its transpose H^T (N x M, pitch ldt)
+//   EPI_GELU_BACK  g = C; dZ = g * gelu'(Z) -> bf16 row-major and transpose
+// gelu(z) = z * Phi(z) (exact, erf); gelu'(z) = Phi(z) + z phi(z).
+// Every mbarrier wait is bounded (2 s) and reports through *status.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "common.cuh"
+#include "tc.cuh"
+
+namespace umapb {
+namespace gemm {
+
+constexpr int BM = 128, BN = 128, BK = 64, UK = 16, STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue (lane quarters 2, 3, 0, 1)
+constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
+
+enum Epi : int { EPI_F32 = 0, EPI_BIAS_GELU = 1, EPI_GELU_BACK = 2 };
+
+struct EpiArgs {
+  int M, N;
+  float* C;  // EPI_F32 output
+  int ldc;
+  const float* bias;      // EPI_BIAS_GELU
+  float* Z;               // EPI_BIAS_GELU output / EPI_GELU_BACK input (pre-activation), pitch ldz
+  int ldz;
+  __nv_bfloat16* H;       // bf16 output (row-major, pitch ldh)
+  int ldh;
+  __nv_bfloat16* HT;      // optional bf16 transposed output (N x M, pitch ldt)
+  int ldt;
+};
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z) {
+  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
+  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
+  return cdf + z * pdf;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int num_kb,
+                EpiArgs e, int32_t* __restrict__ status) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* done = bars + 2 * STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(done, 1);
+    *abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tc::prefetch_tmap(&tmA);
+    tc::prefetch_tmap(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc(tmem_slot, BN);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < num_kb; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+        if (!tc::mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
+        uint8_t* sa = smem + s * STAGE_BYTES;
+        tc::mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+        tc::tma_load_2d(sa, &tmA, &full[s], kb * BK, m0);
+        tc::tma_load_2d(sa + A_BYTES, &tmB, &full[s], kb * BK, n0);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+      bool ok = true;
+      for (int kb = 0; kb < num_kb; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+        if (!tc::mbar_wait(&full[s], ph, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t a_addr = tc::smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+        for (int k = 0; k < BK / UK; ++k)
+          tc::mma_bf16(tmem_base, tc::sw128_kmajor_desc(a_addr + k * 32), tc::sw128_kmajor_desc(b_addr + k * 32),
+                       idesc, (kb | k) != 0 ? 1u : 0u);
+        tc::mma_commit(&empty[s]);
+      }
+      if (ok) tc::mma_commit(done);
+    }
+  } else {
+    // epilogue: thread = accumulator row (TMEM lane), 32 columns per tcgen05.ld
+    const int q = warp & 3;
+    const int r = q * 32 + lane;
+    const int m = m0 + r;
+    if (tc::mbar_wait(done, 0, abort_flag)) {
+      tc::tc_fence_after();
+      for (int ch = 0; ch < BN / 32; ++ch) {
+        float v[32];
+        __syncwarp();
+        tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ch * 32), v);
+        const int nb = n0 + ch * 32;
+        if (m < e.M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int n = nb + j;
+            if (n >= e.N) break;
+            if (EPI == EPI_F32) {
+              e.C[(int64_t)m * e.ldc + n] = v[j];
+            } else if (EPI == EPI_BIAS_GELU) {
+              const float z = v[j] + e.bias[n];
+              e.Z[(int64_t)m * e.ldz + n] = z;
+              const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
+              e.H[(int64_t)m * e.ldh + n] = h;
+              if (e.HT) e.HT[(int64_t)n * e.ldt + m] = h;
+            } else {
+              const float dz = v[j] * gelu_grad(e.Z[(int64_t)m * e.ldz + n]);
+              const __nv_bfloat16 h = __float2bfloat16_rn(dz);
+              e.H[(int64_t)m * e.ldh + n] = h;
+              if (e.HT) e.HT[(int64_t)n * e.ldt + m] = h;
+            }
+          }
+        }
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_base, BN);
+  }
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(status, (int32_t)kDevTimeoutEpilogue);
+}
+
+template <int EPI>
+static int launch(const void* A, const void* B, int M, int N, int K, int lda, int ldb, const EpiArgs& e,
+                  int32_t* status, cudaStream_t stream) {
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr[dev]) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM),
+                   "gemm: smem attribute");
+    attr[dev] = true;
+  }
+  CUtensorMap ta, tb;
+  int s;
+  if ((s = make_tmap_bf16_2d(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, BM, BK))) return s;
+  if ((s = make_tmap_bf16_2d(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, BN, BK))) return s;
+  dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN));
+  gemm_kernel<EPI><<<grid, THREADS, SMEM, stream>>>(ta, tb, (int)ceil_div(K, BK), e, status);
+  UMAPB_LAUNCH_CHECK("gemm kernel launch");
+  count_launches(1);
+  return UMAPB_OK;
+}
+
+}  // namespace gemm
+}  // namespace umapb
+
+using namespace umapb;
+
+extern "C" int umapb_gemm_bf16(const void* A, const void* B, int32_t M, int32_t N, int32_t K, int32_t lda,
+                               int32_t ldb, int32_t epilogue, float* C, int32_t ldc, const float* bias, float* Z,
+                               int32_t ldz, void* H, int32_t ldh, void* HT, int32_t ldt, int32_t* status,
+                               umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(A && B && status, "gemm: null operand");
+  UMAPB_REQUIRE(M >= 1 && N >= 1 && K >= 1, "gemm: empty shape");
+  UMAPB_REQUIRE(lda >= K && ldb >= K && lda % 8 == 0 && ldb % 8 == 0,
+                "gemm: lda/ldb must be >= K and multiples of 8 elements (16-byte rows)");
+  gemm::EpiArgs e{M, N, C, ldc, bias, Z, ldz, static_cast<__nv_bfloat16*>(H), ldh, static_cast<__nv_bfloat16*>(HT),
+                  ldt};
+  switch (epilogue) {
+    case gemm::EPI_F32:
+      UMAPB_REQUIRE(C && ldc >= N, "gemm: EPI_F32 needs C with ldc >= N");
+      return gemm::launch<gemm::EPI_F32>(A, B, M, N, K, lda, ldb, e, status, stream);
+    case gemm::EPI_BIAS_GELU:
+      UMAPB_REQUIRE(bias && Z && H && ldz >= N && ldh >= N && (!HT || ldt >= M),
+                    "gemm: EPI_BIAS_GELU needs bias, Z and H (and ldt >= M for HT)");
+      return gemm::launch<gemm::EPI_BIAS_GELU>(A, B, M, N, K, lda, ldb, e, status, stream);
+    case gemm::EPI_GELU_BACK:
+      UMAPB_REQUIRE(Z && H && ldz >= N && ldh >= N && (!HT || ldt >= M),
+                    "gemm: EPI_GELU_BACK needs Z and H (and ldt >= M for HT)");
+      return gemm::launch<gemm::EPI_GELU_BACK>(A, B, M, N, K, lda, ldb, e, status, stream);
+    default:
+      return set_error(UMAPB_ERR_ARG, "gemm: unknown epilogue %d", epilogue);
+  }
+}

@@ -1,0 +1,227 @@
+"""Learned warm-start encoder for UMAP: an MLP d -> 512 -> 512 -> c with GELU.
+
+New work (the reference initialises UMAP only spectrally or randomly,
+mlx_vis/_umap/umap.py:298-357; its closest idiom is the MMAE MLP trained with
+AdamW, mlx_vis/_mmae/mmae.py:22-38, 258-281).  The encoder regresses UMAP
+embeddings from the input rows.  Used as ``UMAP(init="learned", encoder=enc)``
+it provides the starting layout, so optimize_layout needs fewer epochs, and
+``enc.transform(X_new)`` embeds unseen rows without a fit.
+
+Numerics: FP32 master weights and Adam moments; the two hidden layers run as
+tcgen05 BF16 GEMMs with FP32 accumulation and fused bias + exact GELU
+(libumap_b200 ``umapb_gemm_bf16``); the c-wide output layer keeps FP32 weights.
+The training loss is the mean squared error per row.  Every step is a sequence
+of library kernels (forward, backward, AdamW) — no autograd.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from mlx_vis_b200 import _lib
+from mlx_vis_b200._device import device, to_device_f32, to_host
+from mlx_vis_b200._lib import call, ptr, stream_handle
+
+F32, BIAS_GELU, GELU_BACK = 0, 1, 2
+
+
+def _pad8(x: int) -> int:
+    return (x + 7) // 8 * 8
+
+
+class Encoder:
+    """MLP encoder trained on (X, Y) pairs of UMAP embeddings."""
+
+    def __init__(self, in_dim: int, hidden: int = 512, out_dim: int = 2, lr: float = 1e-3,
+                 weight_decay: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, batch_size: int = 4096,
+                 seed: int = 0):
+        if not 1 <= out_dim <= 4:
+            raise ValueError("out_dim must be between 1 and 4")
+        self.d, self.h, self.c = int(in_dim), int(hidden), int(out_dim)
+        self.lr, self.wd, self.betas, self.eps = lr, weight_decay, betas, eps
+        self.batch_size = int(batch_size)
+        self.seed = seed
+        self.step_count = 0
+        self.dev = device()
+        self.ldx = _pad8(self.d)
+        rng = np.random.default_rng(seed)
+
+        def uniform(shape, fan_in):  # the usual Linear initialisation, U(-1/sqrt(fan_in), 1/sqrt(fan_in))
+            bound = 1.0 / np.sqrt(fan_in)
+            return torch.from_numpy(rng.uniform(-bound, bound, shape).astype(np.float32)).to(self.dev)
+
+        h, d, c = self.h, self.d, self.c
+        self.params = {"W1": uniform((h, d), d), "b1": uniform((h,), d), "W2": uniform((h, h), h),
+                       "b2": uniform((h,), h), "W3": uniform((c, h), h), "b3": uniform((c,), h)}
+        self.m = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.v = {k: torch.zeros_like(v) for k, v in self.params.items()}
+        self.grads = {k: torch.empty_like(v) for k, v in self.params.items()}
+        bf = torch.bfloat16
+        self.W1b = torch.zeros((h, self.ldx), dtype=bf, device=self.dev)
+        self.W2b = torch.empty((h, h), dtype=bf, device=self.dev)
+        self.W2bT = torch.empty((h, h), dtype=bf, device=self.dev)
+        self._refresh_bf16()
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self._buf = {}
+        self.history_ = []
+        self.y_scale_ = None  # (mean, std) of the targets the encoder was trained on
+
+    # ------------------------------------------------------------------
+    def _refresh_bf16(self):
+        p = self.params
+        self.W1b[:, : self.d].copy_(p["W1"].to(torch.bfloat16))
+        self.W2b.copy_(p["W2"].to(torch.bfloat16))
+        self.W2bT.copy_(p["W2"].t().to(torch.bfloat16))
+
+    def _buffers(self, B: int, train: bool):
+        key = (B, train)
+        if key in self._buf:
+            return self._buf[key]
+        dev, bf, h, c = self.dev, torch.bfloat16, self.h, self.c
+        ldb = _pad8(B)
+        b = {"Xb": torch.empty((B, self.ldx), dtype=bf, device=dev), "Z1": torch.empty((B, h), device=dev),
+             "H1": torch.empty((B, h), dtype=bf, device=dev), "Z2": torch.empty((B, h), device=dev),
+             "H2": torch.empty((B, h), dtype=bf, device=dev), "Y": torch.empty((B, c), device=dev), "ldb": ldb}
+        if train:
+            b.update({"XT": torch.zeros((self.d, ldb), dtype=bf, device=dev),
+                      "H1T": torch.zeros((h, ldb), dtype=bf, device=dev),
+                      "H2T": torch.zeros((h, ldb), dtype=bf, device=dev),
+                      "dY": torch.empty((B, c), device=dev), "dZ2": torch.empty((B, h), dtype=bf, device=dev),
+                      "dZ2T": torch.zeros((h, ldb), dtype=bf, device=dev),
+                      "dZ1": torch.empty((B, h), dtype=bf, device=dev),
+                      "dZ1T": torch.zeros((h, ldb), dtype=bf, device=dev),
+                      "loss": torch.zeros(1, device=dev)})
+        self._buf[key] = b
+        return b
+
+    def _gemm(self, A, Bm, M, N, K, lda, ldb, epi, C=None, ldc=0, bias=None, Z=None, ldz=0, H=None, ldh=0, HT=None,
+              ldt=0):
+        call("umapb_gemm_bf16", ptr(A), ptr(Bm), M, N, K, lda, ldb, epi, ptr(C), ldc, ptr(bias), ptr(Z), ldz, ptr(H),
+             ldh, ptr(HT), ldt, ptr(self.status), stream_handle())
+
+    def _forward(self, X: torch.Tensor, b, train: bool):
+        B = X.shape[0]
+        h, p, s = self.h, self.params, stream_handle()
+        call("umapb_mlp_convert", ptr(X), B, self.d, self.ldx, ptr(b["Xb"]), ptr(b["XT"] if train else None),
+             b["ldb"], s)
+        self._gemm(b["Xb"], self.W1b, B, h, self.d, self.ldx, self.ldx, BIAS_GELU, bias=p["b1"], Z=b["Z1"], ldz=h,
+                   H=b["H1"], ldh=h, HT=b["H1T"] if train else None, ldt=b["ldb"])
+        self._gemm(b["H1"], self.W2b, B, h, h, h, h, BIAS_GELU, bias=p["b2"], Z=b["Z2"], ldz=h, H=b["H2"], ldh=h,
+                   HT=b["H2T"] if train else None, ldt=b["ldb"])
+        call("umapb_mlp_head_forward", ptr(b["H2"]), h, B, h, ptr(p["W3"]), ptr(p["b3"]), self.c, ptr(b["Y"]), s)
+        return b["Y"]
+
+    # ------------------------------------------------------------------
+    def train_step(self, X: torch.Tensor, T: torch.Tensor) -> torch.Tensor:
+        """One AdamW step on a batch (device float32 X (B, d), T (B, c)); returns the loss (device)."""
+        X = X.contiguous()
+        T = T.contiguous()
+        B = X.shape[0]
+        h, d, c, p, g = self.h, self.d, self.c, self.params, self.grads
+        b = self._buffers(B, True)
+        s = stream_handle()
+        self._forward(X, b, True)
+        call("umapb_mlp_head_backward", ptr(b["Y"]), ptr(T), B, c, ptr(p["W3"]), h, ptr(b["Z2"]), h, ptr(b["H2T"]),
+             b["ldb"], ptr(b["dY"]), ptr(g["W3"]), ptr(g["b3"]), ptr(b["dZ2"]), h, ptr(b["dZ2T"]), ptr(b["loss"]), s)
+        # dW2 = dZ2^T H1, db2
+        self._gemm(b["dZ2T"], b["H1T"], h, h, B, b["ldb"], b["ldb"], F32, C=g["W2"], ldc=h)
+        call("umapb_mlp_rowsum", ptr(b["dZ2T"]), h, B, b["ldb"], ptr(g["b2"]), s)
+        # dZ1 = (dZ2 W2) * gelu'(Z1)
+        self._gemm(b["dZ2"], self.W2bT, B, h, h, h, h, GELU_BACK, Z=b["Z1"], ldz=h, H=b["dZ1"], ldh=h, HT=b["dZ1T"],
+                   ldt=b["ldb"])
+        # dW1 = dZ1^T X, db1
+        self._gemm(b["dZ1T"], b["XT"], h, d, B, b["ldb"], b["ldb"], F32, C=g["W1"], ldc=d)
+        call("umapb_mlp_rowsum", ptr(b["dZ1T"]), h, B, b["ldb"], ptr(g["b1"]), s)
+        self.step_count += 1
+        self._adamw()
+        return b["loss"]
+
+    def _adamw(self):
+        b1, b2 = self.betas
+        s = stream_handle()
+        for name, prm in self.params.items():
+            rows, cols = (prm.shape[0], prm.shape[1]) if prm.dim() == 2 else (1, prm.shape[0])
+            pb, ldb, pbt, ldbt = None, 0, None, 0
+            if name == "W1":
+                pb, ldb = self.W1b, self.ldx
+            elif name == "W2":
+                pb, ldb, pbt, ldbt = self.W2b, self.h, self.W2bT, self.h
+            call("umapb_adamw", ptr(prm), ptr(self.grads[name]), ptr(self.m[name]), ptr(self.v[name]), rows, cols,
+                 float(self.lr), float(b1), float(b2), float(self.eps), float(self.wd), self.step_count, ptr(pb), ldb,
+                 ptr(pbt), ldbt, s)
+
+    def check_status(self):
+        if int(self.status.item()) != 0:
+            raise _lib.UmapB200Error("umapb_gemm_bf16", 5, "device-side wait expired in a GEMM")
+
+    # ------------------------------------------------------------------
+    def fit(self, Xs, Ys, epochs: int = 20, verbose: bool = False, seed: int = 0):
+        """Trains on the (X, Y) pairs (lists of arrays or tensors); targets are standardised
+        with their global mean / std, which transform() undoes."""
+        Xd = torch.cat([to_device_f32(x, self.dev) for x in Xs])
+        Yd = torch.cat([to_device_f32(y, self.dev) for y in Ys])
+        mean = Yd.mean(dim=0)
+        std = Yd.std(dim=0).clamp_min(1e-6)
+        self.y_scale_ = (mean, std)
+        Yn = ((Yd - mean) / std).contiguous()
+        n = Xd.shape[0]
+        gen = torch.Generator(device=self.dev)
+        gen.manual_seed(seed)
+        B = min(self.batch_size, n)
+        for ep in range(epochs):
+            perm = torch.randperm(n, device=self.dev, generator=gen)
+            total = torch.zeros((), device=self.dev)
+            nb = n // B
+            for i in range(nb):
+                sel = perm[i * B:(i + 1) * B]
+                total += self.train_step(Xd[sel], Yn[sel])[0]
+            self.history_.append(float(total.item()) / max(nb, 1))
+            if verbose:
+                print(f"encoder epoch {ep + 1}/{epochs}: loss {self.history_[-1]:.4f}")
+        self.check_status()
+        return self
+
+    def transform_device(self, X: torch.Tensor, chunk: int = 16384) -> torch.Tensor:
+        """Embeds rows on the device: (n, c) float32 CUDA tensor in the targets' scale."""
+        X = X.contiguous().float()
+        out = torch.empty((X.shape[0], self.c), device=self.dev)
+        for s0 in range(0, X.shape[0], chunk):
+            xb = X[s0:s0 + chunk]
+            b = self._buffers(xb.shape[0], False)
+            out[s0:s0 + xb.shape[0]].copy_(self._forward(xb, b, False))
+        if self.y_scale_ is not None:
+            mean, std = self.y_scale_
+            out = out * std + mean
+        return out
+
+    def transform(self, X) -> np.ndarray:
+        """Out-of-sample embedding of new rows (host float32)."""
+        return to_host(self.transform_device(to_device_f32(X, self.dev)))
+
+    def init_layout(self, Xd: torch.Tensor) -> torch.Tensor:
+        """Starting layout for UMAP(init="learned")."""
+        return self.transform_device(Xd).contiguous()
+
+    # ------------------------------------------------------------------
+    def state_dict(self) -> dict:
+        out = {k: to_host(v) for k, v in self.params.items()}
+        out["config"] = np.array([self.d, self.h, self.c])
+        if self.y_scale_ is not None:
+            out["y_mean"], out["y_std"] = to_host(self.y_scale_[0]), to_host(self.y_scale_[1])
+        return out
+
+    def save(self, path: str) -> None:
+        np.savez(path, **self.state_dict())
+
+    @classmethod
+    def load(cls, path: str, **kw) -> "Encoder":
+        z = np.load(path)
+        d, h, c = (int(v) for v in z["config"])
+        enc = cls(d, hidden=h, out_dim=c, **kw)
+        for k in enc.params:
+            enc.params[k].copy_(torch.from_numpy(z[k]))
+        if "y_mean" in z:
+            enc.y_scale_ = (torch.from_numpy(z["y_mean"]).to(enc.dev), torch.from_numpy(z["y_std"]).to(enc.dev))
+        enc._refresh_bf16()
+        return enc
