@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_FULL, help="rows (default: the 70K workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["fit", "learned_init", "nndescent", "knn_brute", "layout"], default="fit",
+                    help="fit: the benchmark line; learned_init: epochs-to-trustworthiness of the learned warm start; "
+                         "nndescent / knn_brute / layout: one untimed run of that stage (profiler captures)")
     return ap.parse_args()
 
 
@@ -66,7 +69,8 @@ def config(n):
                         f"(n_iters 20, delta 0.015), fuzzy set, spectral init, {N_EPOCHS} epochs, 2 components",
             "n": n, "d": D, "n_neighbors": K_NN, "n_epochs": N_EPOCHS, "min_dist": 0.1, "knn_method": "nndescent",
             "init": "spectral", "parallelism": "replicas (one independent fit per GPU)",
-            "l2": f"inputs larger than L2: X is {n * D * 4 / 1e6:.1f} MB fp32 per step"}
+            "l2": f"inputs larger than L2: every step streams X ({n * D * 4 / 1e6:.1f} MB fp32, above the 126 MB L2) "
+                  "to build its FP16 copy, which evicts the previous step's data"}
 
 
 # --------------------------------------------------------------------------
@@ -138,7 +142,7 @@ def measured_peaks():
 
 def committed_traffic():
     """Per-launch DRAM bytes of the roofline kernel from the committed ncu summary, if any."""
-    path = os.path.join(HERE, "profiles", "nnd_iteration_70k.txt")
+    path = os.path.join(HERE, "profiles", "nnd_iteration_70k.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -282,6 +286,105 @@ def cpu_baseline():
             "stage_s": {k: round(v, 2) for k, v in r["stage_s_full"].items()}, "cpu_s": round(r["cpu_s"], 2)}
 
 
+# --------------------------------------------------------------------------
+LEARNED_TRAIN_SETS, LEARNED_TRAIN_N, LEARNED_EPOCHS = 32, 20000, (25, 50, 100, 200, 300, 500)
+
+
+def run_learned_init(args):
+    """Learned warm start vs spectral init: trustworthiness@15 against layout epochs.
+
+    Encoder trained on 32 seeded 20000x784 prototype mixtures that share their 10
+    prototypes (seeds 1..32, like draws from one image distribution), each embedded
+    with 200 epochs; evaluated on a fresh 70000x784 draw (seed 1000) and on a
+    20000x784 mixture with unseen prototypes.  Trustworthiness on a fixed 10K
+    (5K) row sample, on the GPU.
+    """
+    import torch
+
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import prototype_mixture
+    from mlx_vis_b200.encoder import Encoder
+    from mlx_vis_b200.metrics import trustworthiness
+
+    t0 = time.perf_counter()
+    Xs = [prototype_mixture(LEARNED_TRAIN_N, D, seed=j, proto_seed=0) for j in range(1, LEARNED_TRAIN_SETS + 1)]
+    enc = Encoder.train_on_umap_runs(Xs, n_epochs=200, encoder_epochs=30, seed=0)
+    train_s = time.perf_counter() - t0
+    # encoder step throughput (FLOPs = 6 B (d h + h h + h c) per step)
+    Xd = torch.from_numpy(Xs[0][:4096]).cuda()
+    Td = torch.from_numpy(enc.train_embeddings_[0][:4096]).cuda()
+    for _ in range(5):
+        enc.train_step(Xd, Td)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        enc.train_step(Xd, Td)
+    e1.record()
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / 50
+    flops = 6.0 * 4096 * (D * enc.h + enc.h * enc.h + enc.h * enc.c)
+
+    def trust_curve(X, init, epochs, sub):
+        Xd = torch.from_numpy(X).cuda()
+        out = {}
+        for ne in epochs:
+            u = UMAP(n_epochs=ne, random_state=0, knn_method="nndescent", init=init, encoder=enc)
+            Y = u.fit_transform(Xd)
+            out[ne] = {"trust": round(trustworthiness(X[sub], Y[sub], 15), 5),
+                       "fit_ms": round(u.timings_["total_device"], 2)}
+        return out
+
+    Xt = prototype_mixture(N_FULL, D, seed=1000, proto_seed=0)
+    sub = np.random.default_rng(0).choice(N_FULL, 10000, replace=False)
+    curves = {init: trust_curve(Xt, init, LEARNED_EPOCHS, sub) for init in ("spectral", "learned")}
+    Ytr = enc.transform(Xt)
+    ref = curves["spectral"][500]["trust"]
+    first = {tol: next((ne for ne in LEARNED_EPOCHS if curves["learned"][ne]["trust"] >= ref - tol), None)
+             for tol in (0.005, 0.001)}
+    Xf = prototype_mixture(20000, D, seed=2000, proto_seed=7)
+    subf = np.random.default_rng(1).choice(20000, 5000, replace=False)
+    fresh = {init: trust_curve(Xf, init, (100, 500), subf) for init in ("spectral", "learned")}
+    return {"case": "learned_init", "metric": "trustworthiness@15 vs layout epochs", "unit": "trustworthiness",
+            "config": {"workload": f"encoder {D}->512->512->2 trained on {LEARNED_TRAIN_SETS} x {LEARNED_TRAIN_N}x{D} "
+                                   "prototype mixtures (shared prototypes, 200-epoch UMAP targets); evaluated on a "
+                                   f"fresh {N_FULL}x{D} draw, 10K-row trustworthiness sample"},
+            "train_s": round(train_s, 2), "encoder_step_ms": round(step_ms, 4),
+            "encoder_tflops": round(flops / (step_ms * 1e-3) / 1e12, 1),
+            "curves": curves, "transform_only_trust": round(trustworthiness(Xt[sub], Ytr[sub], 15), 5),
+            "spectral_500": ref,
+            "learned_epochs_to_within": {str(k): v for k, v in first.items()},
+            "epoch_fraction_within_0.005": None if first[0.005] is None else first[0.005] / 500,
+            "unseen_prototypes": fresh}
+
+
+def run_stage(args):
+    """One untimed run of a single stage on its benchmark size, for profiler captures."""
+    import torch
+
+    from mlx_vis_b200 import _lib
+    from mlx_vis_b200._nndescent.nndescent import NNDescent
+
+    if args.case == "knn_brute":
+        from mlx_vis_b200.datasets import prototype_mixture
+
+        Xd = torch.from_numpy(prototype_mixture(20000, D, seed=0)).cuda()
+        idx, d2 = _lib.knn_brute(Xd, K_NN, extra=16)
+        torch.cuda.synchronize()
+        return {"case": "knn_brute", "n": 20000, "d": D, "k": K_NN, "launches": _lib.kernel_launches()}
+    Xd = torch.from_numpy(make_data(args.n)).cuda()
+    if args.case == "nndescent":
+        nn = NNDescent(k=K_NN, random_state=0)
+        nn.build_device(Xd)
+        torch.cuda.synchronize()
+        return {"case": "nndescent", "n": args.n, "iterations": len(nn.history_), "launches": _lib.kernel_launches()}
+    from mlx_vis_b200 import UMAP
+
+    UMAP(n_components=2, n_neighbors=K_NN, n_epochs=N_EPOCHS, knn_method="nndescent", random_state=0,
+         use_graph=False).fit_transform_device(Xd)
+    torch.cuda.synchronize()
+    return {"case": "layout", "n": args.n, "launches": _lib.kernel_launches()}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
@@ -311,6 +414,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         out = run_reference(args, rank)
+    elif args.case == "learned_init":
+        out = run_learned_init(args) if rank == 0 else None
+    elif args.case != "fit":
+        out = run_stage(args) if rank == 0 else None
     else:
         out = run_ours(args, rank, world, local_rank)
     if out is not None and rank == 0:

@@ -204,6 +204,40 @@ class Encoder:
         return self.transform_device(Xd).contiguous()
 
     # ------------------------------------------------------------------
+    @classmethod
+    def train_on_umap_runs(cls, Xs, n_epochs: int = 200, encoder_epochs: int = 30, finetune_epochs: int = 5,
+                           seed: int = 0, umap_kwargs=None, **kw) -> "Encoder":
+        """Trains an encoder on UMAP embeddings of the datasets ``Xs`` (same feature space).
+
+        UMAP layouts are defined only up to rotation and reflection, so independent runs
+        give targets that disagree with each other.  The runs are therefore chained: the
+        first dataset is embedded with the plain (spectral) initialisation, every later
+        one with ``init="learned"`` from the encoder trained so far (fine-tuned on each new
+        run for ``finetune_epochs``), which keeps all layouts in one orientation.  A fresh
+        encoder is then fitted on all pairs for ``encoder_epochs``.
+        """
+        from mlx_vis_b200._umap.umap import UMAP
+
+        uk = dict(umap_kwargs or {})
+        uk.setdefault("knn_method", "nndescent")
+        kw.setdefault("out_dim", uk.get("n_components", 2))
+        d = int(np.asarray(Xs[0]).shape[1]) if not torch.is_tensor(Xs[0]) else int(Xs[0].shape[1])
+        pairs_x, pairs_y = [], []
+        enc = None
+        for j, X in enumerate(Xs):
+            if enc is None:
+                Y = UMAP(n_epochs=n_epochs, random_state=seed + j, **uk).fit_transform(X)
+                enc = cls(d, seed=seed, **kw).fit([X], [Y], epochs=encoder_epochs)
+            else:
+                Y = UMAP(n_epochs=n_epochs, random_state=seed + j, init="learned", encoder=enc, **uk).fit_transform(X)
+                enc.fit([X], [Y], epochs=finetune_epochs)
+            pairs_x.append(X)
+            pairs_y.append(Y)
+        final = cls(d, seed=seed, **kw).fit(pairs_x, pairs_y, epochs=encoder_epochs)
+        final.train_embeddings_ = pairs_y
+        return final
+
+    # ------------------------------------------------------------------
     def state_dict(self) -> dict:
         out = {k: to_host(v) for k, v in self.params.items()}
         out["config"] = np.array([self.d, self.h, self.c])

@@ -127,3 +127,22 @@ def test_gpu_trustworthiness_equals_sklearn():
     X = rng.normal(size=(700, 20))
     Y = X[:, :2] + 0.3 * rng.normal(size=(700, 2))
     assert abs(trustworthiness(X, Y, 15) - sk_tw(X, Y, n_neighbors=15)) < 1e-9
+
+
+def test_learned_init_matches_full_run_trust_in_40pct_of_epochs():
+    """Warm start from an encoder trained on other draws of the same distribution:
+    200 layout epochs (40%) reach the trustworthiness of a 500-epoch spectral run."""
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import prototype_mixture
+    from mlx_vis_b200.encoder import Encoder
+    from mlx_vis_b200.metrics import trustworthiness
+
+    Xs = [prototype_mixture(5000, 784, seed=j, proto_seed=0) for j in range(1, 5)]
+    enc = Encoder.train_on_umap_runs(Xs, n_epochs=200, encoder_epochs=30, umap_kwargs={"knn_method": "brute"})
+    Xt = prototype_mixture(10000, 784, seed=100, proto_seed=0)
+    sub = np.random.default_rng(0).choice(10000, 4000, replace=False)
+    full = UMAP(n_epochs=500, random_state=0).fit_transform(Xt)
+    warm = UMAP(n_epochs=200, random_state=0, init="learned", encoder=enc).fit_transform(Xt)
+    t_full = trustworthiness(Xt[sub], full[sub], 15)
+    t_warm = trustworthiness(Xt[sub], warm[sub], 15)
+    assert t_warm >= t_full - 0.005, (t_warm, t_full)
