@@ -108,6 +108,14 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     *evals (device uint64, nullable) += distances evaluated.
  *                     Rows without a NEW flag are copied on the converging path.
  * umapb_nnd_sqrt:     Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400).
+ * umapb_nnd_random_start: the reference's random start drawn on the device
+ *                     (nndescent.py:47-57, 72-82): from the NumPy legacy state in
+ *                     `state` (device uint32[628]: MT19937 key[624], pos,
+ *                     has_gauss, gauss as a double, low word first — the layout of
+ *                     np.random.get_state()), idx (n, k) = randint(0, n - 1)
+ *                     shifted past the row index, then P (d, pd1) and P2 (d, pd2) =
+ *                     float32(float32(randn) / sqrt(pd)) for pd > 0 (0 skips the
+ *                     draw); `state` is overwritten with the state after the draws.
  * ------------------------------------------------------------------------- */
 int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq, umapb_stream_t stream);
 int umapb_nnd_to_half(const float* X, int64_t count, void* H, umapb_stream_t stream);
@@ -122,6 +130,8 @@ int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ha
                         float* dist_new, uint8_t* flags_new, unsigned long long* changed,
                         unsigned long long* evals, umapb_stream_t stream);
 int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_stream_t stream);
+int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P, int32_t pd1,
+                           float* P2, int32_t pd2, umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Fuzzy simplicial set — replaces UMAP._fuzzy_simplicial_set

@@ -55,6 +55,7 @@ SIGNATURES = {
     "umapb_mlp_rowsum": [_p, _i32, _i32, _i32, _p, _p],
     "umapb_adamw": [_p, _p, _p, _p, _i32, _i32, _f32, _f32, _f32, _f32, _f32, _i32, _p, _i32, _p, _i32, _p],
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
+    "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],

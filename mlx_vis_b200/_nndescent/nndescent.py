@@ -5,7 +5,10 @@ The control flow is the reference's, kept on the host:
 * the same random draws from NumPy's global stream: ``np.random.seed``,
   ``randint(0, n-1, (n, k))`` shifted past self, then the two projections
   ``randn(d, 100)/sqrt(100)`` and ``randn(d, 300)/sqrt(300)`` (nndescent.py:47-82),
-  so the random start and the projections are identical to the reference's;
+  so the random start and the projections are identical to the reference's.
+  The draws are made on the device from the stream's state (MT19937, masked
+  rejection, polar normals; random_start.cu) and the advanced state is handed
+  back to NumPy, which leaves the global stream where the reference leaves it;
 * per iteration mc_nn / j_nn from the update fraction (nndescent.py:100-101);
 * full path while the update fraction is >= 0.5: iteration 0 in the 100-d
   projection, iteration 1 in the 300-d projection, FP16 distances in iterations
@@ -44,8 +47,45 @@ def iteration_params(update_frac: float, k: int, mc: int):
     return min(mc_nn, k), j_nn, min(mc_conv, k)
 
 
+def state_words(state) -> np.ndarray:
+    """np.random.get_state() as the uint32[628] buffer umapb_nnd_random_start reads."""
+    name, key, pos, has_gauss, gauss = state[:5]
+    if name != "MT19937":
+        raise ValueError("NumPy's global stream is not MT19937")
+    w = np.empty(628, dtype=np.uint32)
+    w[:624] = key
+    w[624], w[625] = pos, has_gauss
+    w[626:] = np.array([gauss], dtype=np.float64).view(np.uint32)
+    return w
+
+
+def words_state(w: np.ndarray):
+    """The inverse of state_words, for np.random.set_state."""
+    w = np.asarray(w, dtype=np.uint32)
+    return ("MT19937", w[:624].copy(), int(w[624]), int(w[625]), float(w[626:628].view(np.float64)[0]))
+
+
+def random_start_device(n: int, k: int, d: int, random_state, dev):
+    """The reference's draws made on the device (umapb_nnd_random_start).
+
+    Seeds NumPy's global stream like the reference, hands its state to the
+    kernel and returns (idx, P, P2, state) with ``state`` the device buffer that
+    holds the stream's state after the draws (give it back with
+    ``np.random.set_state(words_state(state.cpu().numpy()))``)."""
+    if random_state is not None:
+        np.random.seed(random_state)
+    state = torch.from_numpy(state_words(np.random.get_state())).to(dev)
+    pd1, pd2 = min(100, d), min(300, d)
+    idx = torch.empty((n, k), dtype=torch.int32, device=dev)
+    P = torch.empty((d, pd1), dtype=torch.float32, device=dev) if pd1 < d else None
+    P2 = torch.empty((d, pd2), dtype=torch.float32, device=dev) if pd2 < d else None
+    call("umapb_nnd_random_start", ptr(state), n, k, d, ptr(idx), ptr(P), pd1 if P is not None else 0, ptr(P2),
+         pd2 if P2 is not None else 0, stream_handle())
+    return idx, P, P2, state
+
+
 def random_start(n: int, k: int, d: int, random_state):
-    """The reference's draws, in its order (nndescent.py:47-57, 72-82)."""
+    """The reference's draws on the host, in its order (nndescent.py:47-57, 72-82)."""
     if random_state is not None:
         np.random.seed(random_state)
     idx = np.random.randint(0, n - 1, (n, k), dtype=np.int32)
@@ -100,8 +140,7 @@ class NNDescent:
         _lib.load()
         s = stream_handle()
 
-        idx_h, P, P2 = random_start(n, k, d, self.random_state)
-        idx = torch.from_numpy(idx_h).to(dev, non_blocking=True)
+        idx, P, P2, rng_state = random_start_device(n, k, d, self.random_state, dev)
         dist = torch.empty((n, k), dtype=torch.float32, device=dev)
         sq = torch.empty(n, dtype=torch.float32, device=dev)
         call("umapb_nnd_sqnorms", ptr(X), n, d, 0, ptr(sq), s)
@@ -109,12 +148,12 @@ class NNDescent:
 
         if P is not None:
             with _no_tf32():
-                X_low = (X @ torch.from_numpy(P).to(dev)).contiguous()
+                X_low = (X @ P).contiguous()
             sq_low = torch.empty(n, dtype=torch.float32, device=dev)
             call("umapb_nnd_sqnorms", ptr(X_low), n, X_low.shape[1], 0, ptr(sq_low), s)
         else:
             X_low, sq_low = X, sq
-        P2_d = torch.from_numpy(P2).to(dev) if P2 is not None else None
+        P2_d = P2
 
         rev = torch.empty((n, k), dtype=torch.int32, device=dev)
         rev_ws = _lib.workspace(query("umapb_nnd_reverse_workspace", n, k), dev)
@@ -196,6 +235,7 @@ class NNDescent:
                 if self.verbose:
                     print(f"Converged at iteration {it + 1}")
                 break
+        np.random.set_state(words_state(rng_state.cpu().numpy()))
         out = torch.empty_like(dist)
         _sqrt_into(dist, out)
         return idx, out

@@ -37,8 +37,13 @@ constexpr int kEdgesPerBlock = 1024;
 
 // ---- reference pair math (float32, evaluation order of umap.py:361-383) ----
 struct Params {
-  float a, b, bm1, two_b, alpha;
+  float a, b, m2ab, two_b, alpha;
 };
+
+// d^(2b) is evaluated once per pair as exp2(b log2 d2) (CUDA's log2f / exp2f, a few
+// ulp); d^(2(b-1)) = d^(2b) / d2.  The reference evaluates mx.power twice in float32;
+// the difference is a few float32 ulp of the coefficient.
+__device__ __forceinline__ float pow_b(float d2, float b) { return exp2f(__fmul_rn(b, log2f(d2))); }
 
 template <int DIM>
 __device__ __forceinline__ void attract(const float (&yi)[DIM], const float (&yj)[DIM], const Params& p,
@@ -51,9 +56,9 @@ __device__ __forceinline__ void attract(const float (&yi)[DIM], const float (&yj
     d2 = __fadd_rn(d2, __fmul_rn(diff[c], diff[c]));
   }
   d2 = fmaxf(d2, 1e-6f);
-  const float pw = powf(d2, p.b);
-  const float num = __fmul_rn(__fmul_rn(__fmul_rn(-2.0f, p.a), p.b), powf(d2, p.bm1));
-  const float coeff = __fdiv_rn(num, __fadd_rn(1.0f, __fmul_rn(p.a, pw)));
+  const float pw = pow_b(d2, p.b);
+  // -2ab d^(2(b-1)) / (1 + a d^(2b)) = (-2ab) d^(2b) / (d2 (1 + a d^(2b)))
+  const float coeff = __fdiv_rn(__fmul_rn(p.m2ab, pw), __fmul_rn(d2, __fadd_rn(1.0f, __fmul_rn(p.a, pw))));
 #pragma unroll
   for (int c = 0; c < DIM; ++c) out[c] = __fmul_rn(fminf(fmaxf(__fmul_rn(coeff, diff[c]), -4.0f), 4.0f), p.alpha);
 }
@@ -69,7 +74,7 @@ __device__ __forceinline__ void repel_add(const float (&yi)[DIM], const float (&
     d2 = __fadd_rn(d2, __fmul_rn(diff[c], diff[c]));
   }
   d2 = fmaxf(d2, 1e-6f);
-  const float pw = powf(d2, p.b);
+  const float pw = pow_b(d2, p.b);
   const float den = __fmul_rn(__fadd_rn(0.001f, d2), __fadd_rn(1.0f, __fmul_rn(p.a, pw)));
   const float coeff = __fdiv_rn(p.two_b, den);
 #pragma unroll
@@ -133,6 +138,43 @@ __global__ void eps_kernel(const float* __restrict__ vals, const int64_t* __rest
 }
 
 // ---- fast path epoch ---------------------------------------------------------
+// Only the edges due in an epoch do work, about a third of them on average, so a
+// thread-per-edge loop leaves most lanes idle.  Each warp scans a contiguous
+// segment of edges, advances the schedule of the due ones and queues them in
+// shared memory; the warp works through the queue 32 edges at a time with every
+// lane busy (at most one partial batch per warp, at the end of its segment).
+template <int DIM>
+__device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* __restrict__ dY, int n,
+                                            const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
+                                            int64_t e, int epoch, const Params& p, int neg_rate, uint32_t k0,
+                                            uint32_t k1) {
+  const int i = rows[e], j = cols[e];
+  float yi[DIM], yj[DIM], acc[DIM], pos[DIM], neg_pos[DIM];
+  load_row<DIM>(Y, i, yi);
+  load_row<DIM>(Y, j, yj);
+  attract<DIM>(yi, yj, p, pos);
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    acc[c] = pos[c];
+    neg_pos[c] = -pos[c];
+  }
+  atomic_add_row<DIM>(dY, j, neg_pos);
+  auto repel = [&](uint32_t r) {
+    float yt[DIM];
+    load_row<DIM>(Y, to_range(r, (uint32_t)n), yt);
+    repel_add<DIM>(yi, yt, p, acc);
+  };
+#pragma unroll 1
+  for (int m0 = 0; m0 < neg_rate; m0 += 4) {
+    const U4 r = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, (uint32_t)(m0 >> 2)}, k0, k1);
+    repel(r.x);
+    if (m0 + 1 < neg_rate) repel(r.y);
+    if (m0 + 2 < neg_rate) repel(r.z);
+    if (m0 + 3 < neg_rate) repel(r.w);
+  }
+  atomic_add_row<DIM>(dY, i, acc);
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(kBlock) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY, int n,
                                                            const int32_t* __restrict__ rows,
@@ -140,38 +182,39 @@ __global__ void __launch_bounds__(kBlock) sgd_epoch_kernel(const float* __restri
                                                            const float* __restrict__ eps, float* __restrict__ next,
                                                            const int64_t* __restrict__ n_edges, int epoch, Params p,
                                                            int neg_rate, uint32_t k0, uint32_t k1) {
+  __shared__ int32_t queue[kBlock / 32][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int32_t* q = queue[warp];
   const int64_t E = *n_edges;
   const float ep = (float)epoch;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
-    const float nx = next[e];
-    if (!(nx <= ep)) continue;
-    next[e] = __fadd_rn(nx, eps[e]);
-    const int i = rows[e], j = cols[e];
-    float yi[DIM], yj[DIM], acc[DIM], pos[DIM];
-    load_row<DIM>(Y, i, yi);
-    load_row<DIM>(Y, j, yj);
-    attract<DIM>(yi, yj, p, pos);
-    float neg_pos[DIM];
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      acc[c] = pos[c];
-      neg_pos[c] = -pos[c];
+  const int64_t n_warps = (int64_t)gridDim.x * (kBlock / 32);
+  const int64_t seg = (((E + 31) / 32 + n_warps - 1) / n_warps) * 32;
+  const int64_t e0 = ((int64_t)blockIdx.x * (kBlock / 32) + warp) * seg;
+  const int64_t e1 = e0 + seg < E ? e0 + seg : E;
+  const unsigned below = (1u << lane) - 1u;
+  int cnt = 0;  // queued edges (offsets from e0), < 32 between batches
+  for (int64_t base = e0; base < e1; base += 32) {
+    const int64_t e = base + lane;
+    bool due = false;
+    if (e < e1) {
+      const float nx = next[e];
+      due = nx <= ep;
+      if (due) next[e] = __fadd_rn(nx, eps[e]);
     }
-    atomic_add_row<DIM>(dY, j, neg_pos);
-    for (int m0 = 0; m0 < neg_rate; m0 += 4) {
-      const U4 r = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, (uint32_t)(m0 >> 2)}, k0, k1);
-      const uint32_t rs[4] = {r.x, r.y, r.z, r.w};
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (m0 + u < neg_rate) {
-          float yt[DIM];
-          load_row<DIM>(Y, to_range(rs[u], (uint32_t)n), yt);
-          repel_add<DIM>(yi, yt, p, acc);
-        }
-      }
+    const unsigned b = __ballot_sync(0xffffffffu, due);
+    if (due) q[cnt + __popc(b & below)] = (int32_t)(e - e0);
+    cnt += __popc(b);
+    __syncwarp();
+    if (cnt >= 32) {
+      const int64_t my = e0 + q[lane];
+      __syncwarp();
+      if (lane < cnt - 32) q[lane] = q[lane + 32];
+      cnt -= 32;
+      __syncwarp();
+      edge_update<DIM>(Y, dY, n, rows, cols, my, epoch, p, neg_rate, k0, k1);
     }
-    atomic_add_row<DIM>(dY, i, acc);
   }
+  if (lane < cnt) edge_update<DIM>(Y, dY, n, rows, cols, e0 + q[lane], epoch, p, neg_rate, k0, k1);
 }
 
 __global__ void apply_kernel(float* __restrict__ Y, float* __restrict__ dY, int64_t m) {
@@ -286,7 +329,7 @@ static Params make_params(float a, float b, float lr, int epoch, int n_epochs) {
   Params p;
   p.a = a;
   p.b = b;
-  p.bm1 = b - 1.0f;
+  p.m2ab = (-2.0f * a) * b;
   p.two_b = 2.0f * b;
   // the reference computes alpha in Python double and casts it to float32 (umap.py:431)
   p.alpha = (float)((double)lr * (1.0 - (double)epoch / (double)n_epochs));
@@ -299,11 +342,18 @@ static unsigned edge_grid(int64_t e_cap) {
   return (unsigned)(want < cap ? want : cap);
 }
 
+// a few resident blocks per SM: long warp segments keep the partial batches rare
+static unsigned epoch_grid(int64_t e_cap) {
+  const int64_t want = ceil_div(e_cap > 0 ? e_cap : 1, kBlock * 4);
+  const int64_t cap = (int64_t)num_sms() * 4;
+  return (unsigned)(want < cap ? want : cap);
+}
+
 template <int DIM>
 static void launch_epoch(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
                          const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
                          const Params& p, int neg_rate, uint64_t seed, cudaStream_t stream) {
-  sgd_epoch_kernel<DIM><<<edge_grid(e_cap), kBlock, 0, stream>>>(Y, l.dY, (int)n, rows, cols, eps, next, n_edges,
+  sgd_epoch_kernel<DIM><<<epoch_grid(e_cap), kBlock, 0, stream>>>(Y, l.dY, (int)n, rows, cols, eps, next, n_edges,
                                                                  epoch, p, neg_rate, (uint32_t)seed,
                                                                  (uint32_t)(seed >> 32));
   const int64_t m = n * DIM;

@@ -8,6 +8,7 @@ within a fraction of a percent and the per-iteration change counts track."""
 
 import numpy as np
 import pytest
+import torch
 
 from oracle import knn as oknn
 from oracle import nndescent as onnd
@@ -95,3 +96,54 @@ def test_umap_with_nndescent(gauss2000):
 
     Y = UMAP(n_epochs=200, knn_method="nndescent", random_state=0).fit_transform(gauss2000)
     assert trustworthiness(gauss2000, Y, n_neighbors=15) > 0.95
+
+
+@pytest.mark.parametrize("n,k,d,seed", [(70000, 15, 784, 0), (5000, 15, 784, 3), (1000, 10, 150, 7), (257, 4, 64, 1),
+                                        (2, 1, 5, 2), (3000, 32, 301, 11)])
+def test_device_random_start_equals_numpy(n, k, d, seed):
+    """umapb_nnd_random_start reproduces the reference's NumPy draws bit for bit
+    and leaves NumPy's global stream in the same state."""
+    from mlx_vis_b200._nndescent.nndescent import random_start, random_start_device, words_state
+
+    idx_h, P_h, P2_h = random_start(n, k, d, seed)
+    st_h = np.random.get_state()
+    idx, P, P2, state = random_start_device(n, k, d, seed, torch.device("cuda"))
+    st = words_state(state.cpu().numpy())
+    assert np.array_equal(idx.cpu().numpy(), idx_h)
+    for got, want in ((P, P_h), (P2, P2_h)):
+        assert (got is None) == (want is None)
+        if got is not None:
+            assert np.array_equal(got.cpu().numpy(), want)
+    assert np.array_equal(st[1], st_h[1]) and st[2:] == st_h[2:]
+
+
+def test_device_random_start_continues_an_unseeded_stream():
+    """random_state=None: the draws continue NumPy's global stream, including a
+    cached second normal (has_gauss) and a mid-generation position."""
+    from mlx_vis_b200._nndescent.nndescent import random_start, random_start_device, words_state
+
+    np.random.seed(5)
+    np.random.randn(3)  # leaves a cached normal
+    np.random.randint(0, 10, 7)
+    st0 = np.random.get_state()
+    assert st0[3] == 1
+    idx_h, P_h, P2_h = random_start(900, 6, 350, None)
+    st_h = np.random.get_state()
+    np.random.set_state(st0)
+    idx, P, P2, state = random_start_device(900, 6, 350, None, torch.device("cuda"))
+    st = words_state(state.cpu().numpy())
+    assert np.array_equal(idx.cpu().numpy(), idx_h)
+    assert np.array_equal(P.cpu().numpy(), P_h) and np.array_equal(P2.cpu().numpy(), P2_h)
+    assert np.array_equal(st[1], st_h[1]) and st[2:] == st_h[2:]
+
+
+def test_build_leaves_numpy_stream_like_the_reference():
+    from mlx_vis_b200 import NNDescent
+    from mlx_vis_b200._nndescent.nndescent import random_start
+
+    X = np.random.default_rng(0).normal(size=(600, 40)).astype(np.float32)
+    NNDescent(k=8, random_state=4).build(X)
+    after = np.random.get_state()
+    random_start(600, 8, 40, 4)
+    want = np.random.get_state()
+    assert np.array_equal(after[1], want[1]) and after[2:] == want[2:]

@@ -88,3 +88,24 @@ def test_fit_without_gpu_fails_loudly(monkeypatch):
     monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
     with pytest.raises(RuntimeError, match="CUDA device"):
         UMAP().fit_transform(np.zeros((10, 3), dtype=np.float32))
+
+
+@pytest.mark.parametrize("n,k,d,seed", [(50, 5, 120, 3), (300, 15, 400, 7), (2, 1, 5, 1), (1000, 15, 101, 0)])
+def test_mt19937_restatement_matches_numpy(n, k, d, seed):
+    """The oracle's MT19937 / masked-rejection / polar-normal restatement (the
+    checker of the device random start) reproduces NumPy's legacy draws and state."""
+    from mlx_vis_b200._nndescent.nndescent import random_start, state_words, words_state
+    from oracle import mt19937
+
+    np.random.seed(seed)
+    st0 = np.random.get_state()
+    idx, P, P2, st = mt19937.random_start(st0, n, k, d)
+    idx_h, P_h, P2_h = random_start(n, k, d, seed)
+    st_h = np.random.get_state()
+    assert np.array_equal(idx, idx_h)
+    for a, b in ((P, P_h), (P2, P2_h)):
+        assert (a is None and b is None) or np.array_equal(a, b)
+    assert np.array_equal(st[1], st_h[1]) and st[2:] == st_h[2:]
+    # the uint32 state buffer of umapb_nnd_random_start round-trips
+    back = words_state(state_words(st_h))
+    assert np.array_equal(back[1], st_h[1]) and back[2:] == st_h[2:]
