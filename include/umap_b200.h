@@ -88,7 +88,9 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  * NNDescent — replaces NNDescent.build (mlx_vis/_nndescent/nndescent.py:34-403);
  * the host keeps the reference's iteration control and random draws.  k <= 32.
  * umapb_nnd_sqnorms:  sq[i] = |X_i|^2 (X float32, or FP16 when half != 0).
- * umapb_nnd_to_half:  FP16 copy of an FP32 array (the FP16 iterations 1-4).
+ * umapb_nnd_to_half:  FP16 copy of (n, dd) FP32 rows into rows of pitch ldh >= dd
+ *                     (zero padded; the FP16 iterations 1-4 use ldh = dd rounded
+ *                     up to a multiple of 8).
  * umapb_nnd_gather:   dist[i][p] = max(sq_i + sq_j - 2 X_i.X_j, 0) for j = idx[i][p]
  *                     in FP32 (_gather_dists, nndescent.py:573-612); with
  *                     sort_rows != 0 each row is then sorted by (distance, id)
@@ -100,8 +102,9 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     103-217 converging path): candidates [idx row | first j_nn
  *                     of the rows of its first mc_new neighbours (NEW first when
  *                     converging) | rev row], first occurrence of a duplicate kept,
- *                     distances in the space Xd (FP16 dot products rounded to FP16
- *                     when half != 0), stored distances reused for current
+ *                     distances in the space Xd (rows of dd values at a pitch of
+ *                     ldx; FP16 rows need ldx % 8 == 0 and zero padding; FP16
+ *                     dot products are rounded to FP16 when half != 0), stored distances reused for current
  *                     neighbours unless recompute_cur, self and duplicates 1e30,
  *                     the k smallest (distance, id) kept; flags_new = positional
  *                     change flags, *changed (device uint64) += their count,
@@ -118,13 +121,13 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     draw); `state` is overwritten with the state after the draws.
  * ------------------------------------------------------------------------- */
 int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq, umapb_stream_t stream);
-int umapb_nnd_to_half(const float* X, int64_t count, void* H, umapb_stream_t stream);
+int umapb_nnd_to_half(const float* X, int64_t n, int32_t dd, int32_t ldh, void* H, umapb_stream_t stream);
 int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int32_t dd, int32_t* idx, float* dist, int32_t k,
                      int32_t sort_rows, umapb_stream_t stream);
 int umapb_nnd_reverse_workspace(int64_t n, int32_t k, size_t* bytes);
 int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, void* workspace,
                       size_t workspace_bytes, umapb_stream_t stream);
-int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t half, const int32_t* idx_old,
+int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
                         const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n, int32_t k,
                         int32_t mc_new, int32_t j_nn, int32_t converging, int32_t recompute_cur, int32_t* idx_new,
                         float* dist_new, uint8_t* flags_new, unsigned long long* changed,
@@ -132,6 +135,12 @@ int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ha
 int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_stream_t stream);
 int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P, int32_t pd1,
                            float* P2, int32_t pd2, umapb_stream_t stream);
+/* umapb_legacy_normal: count values float32(loc + scale * g) with g NumPy's legacy
+ * standard normals drawn from `state` (same buffer layout as above; overwritten
+ * with the state after the draws) — RandomState(seed).normal(loc, scale, count)
+ * cast to float32, as the spectral init's noise (umap.py:344-346). */
+int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out,
+                        umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Fuzzy simplicial set — replaces UMAP._fuzzy_simplicial_set

@@ -18,7 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libumap_b200.so")
 
 _c = ctypes
-_i32, _i64, _u64, _f32, _sz = _c.c_int32, _c.c_int64, _c.c_uint64, _c.c_float, _c.c_size_t
+_i32, _i64, _u64, _f32, _f64, _sz = _c.c_int32, _c.c_int64, _c.c_uint64, _c.c_float, _c.c_double, _c.c_size_t
 _p = _c.c_void_p
 _psz = _c.POINTER(_c.c_size_t)
 
@@ -40,12 +40,12 @@ SIGNATURES = {
     "umapb_layout_epochs": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32,
                             _u64, _p, _sz, _p],
     "umapb_nnd_sqnorms": [_p, _i64, _i32, _i32, _p, _p],
-    "umapb_nnd_to_half": [_p, _i64, _p, _p],
+    "umapb_nnd_to_half": [_p, _i64, _i32, _i32, _p, _p],
     "umapb_nnd_gather": [_p, _p, _i64, _i32, _p, _p, _i32, _i32, _p],
     "umapb_nnd_reverse_workspace": [_i64, _i32, _psz],
     "umapb_nnd_reverse": [_p, _i64, _i32, _p, _p, _sz, _p],
-    "umapb_nnd_iteration": [_p, _p, _i32, _i32, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _i32, _i32, _p, _p, _p, _p,
-                            _p, _p],
+    "umapb_nnd_iteration": [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _i32, _i32, _p, _p,
+                            _p, _p, _p, _p],
     "umapb_kernel_launches": [],
     "umapb_gemm_bf16": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _p, _i32, _p, _p, _i32, _p, _i32, _p, _i32, _p,
                         _p],
@@ -56,6 +56,7 @@ SIGNATURES = {
     "umapb_adamw": [_p, _p, _p, _p, _i32, _i32, _f32, _f32, _f32, _f32, _f32, _i32, _p, _i32, _p, _i32, _p],
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
     "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p],
+    "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],
@@ -192,6 +193,17 @@ def normal(shape, seed: int, device) -> torch.Tensor:
     """Standard normal float32 tensor drawn by the library's Philox kernel."""
     out = torch.empty(shape, dtype=torch.float32, device=device)
     call("umapb_normal_fill", ptr(out), out.numel(), int(seed) & 0xFFFFFFFFFFFFFFFF, stream_handle())
+    return out
+
+
+def legacy_normal(rs, shape, loc: float, scale: float, device) -> torch.Tensor:
+    """float32(rs.normal(loc, scale, shape)) for a NumPy RandomState ``rs``, drawn on
+    the device from rs's state (umapb_legacy_normal); ``rs`` itself is not advanced."""
+    from mlx_vis_b200._nndescent.nndescent import state_words
+
+    state = torch.from_numpy(state_words(rs.get_state())).to(device)
+    out = torch.empty(shape, dtype=torch.float32, device=device)
+    call("umapb_legacy_normal", ptr(state), out.numel(), float(loc), float(scale), ptr(out), stream_handle())
     return out
 
 

@@ -180,7 +180,7 @@ class NNDescent:
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
                 ev[0].record() if ev else None
-                call("umapb_nnd_iteration", ptr(X), ptr(sq), d, 0, ptr(idx), ptr(dist), ptr(flags),
+                call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
                      ptr(rev if use_rev else None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2),
                      ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
@@ -198,19 +198,21 @@ class NNDescent:
                 use_half = it in (1, 2, 3, 4)
                 recompute = (it == 0) or use_half
                 dd = Xd.shape[1]
+                ldx = dd
                 if use_half:
+                    ldx = (dd + 7) // 8 * 8  # FP16 rows padded to 16-byte chunks
                     if Xd is X:
                         if Xh is None:
-                            Xh = torch.empty((n, d), dtype=torch.float16, device=dev)
-                            call("umapb_nnd_to_half", ptr(X), n * d, ptr(Xh), s)
+                            Xh = torch.empty((n, ldx), dtype=torch.float16, device=dev)
+                            call("umapb_nnd_to_half", ptr(X), n, d, ldx, ptr(Xh), s)
                         src = Xh
                     else:
-                        src = torch.empty((n, dd), dtype=torch.float16, device=dev)
-                        call("umapb_nnd_to_half", ptr(Xd), n * dd, ptr(src), s)
+                        src = torch.empty((n, ldx), dtype=torch.float16, device=dev)
+                        call("umapb_nnd_to_half", ptr(Xd), n, dd, ldx, ptr(src), s)
                 else:
                     src = Xd
                 ev[0].record() if ev else None
-                call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, int(use_half), ptr(idx), ptr(dist), ptr(None),
+                call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
                      ptr(rev if use_rev else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2), ptr(dist2),
                      ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None

@@ -148,6 +148,7 @@ class UMAP:
         self._optimize(rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback)
         ev.mark("layout")
         self.timings_ = ev.finish()
+        self.graph_ = None  # the replay has finished; release the graph and its memory pool
         self.graph_info_ = {"n_edges": int(n_edges.item())}
         return Y
 
@@ -178,9 +179,9 @@ class UMAP:
             raise ValueError(f"unknown init {self.init!r}")
         try:
             V0 = _lib.normal((n, c + 1), seed, dev)
-            rng = np.random.RandomState(self.random_state or 42)
-            noise = rng.normal(scale=0.0001, size=(n, c)).astype(np.float32)
-            noise_d = torch.from_numpy(noise).to(dev, non_blocking=True)
+            # RandomState(random_state or 42).normal(scale=1e-4, size=(n, c)) as float32
+            # (umap.py:344-346), drawn on the device from that stream's state
+            noise_d = _lib.legacy_normal(np.random.RandomState(self.random_state or 42), (n, c), 0.0, 0.0001, dev)
             Y = _lib.spectral(rows, cols, vals, n_edges, n, c, V0, noise_d, n_iter=100)
             if self.verbose:
                 print("Using spectral initialization")

@@ -124,9 +124,14 @@ __global__ void sqnorm_kernel(const T* __restrict__ X, int64_t n, int dd, float*
   if (lane == 0) sq[row] = acc;
 }
 
-__global__ void to_half_kernel(const float* __restrict__ X, int64_t m, __half* __restrict__ H) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
-    H[t] = __float2half_rn(X[t]);
+// FP16 copy of (n, dd) FP32 rows into rows of pitch ldh >= dd, zero padded
+__global__ void to_half_kernel(const float* __restrict__ X, int64_t n, int dd, int ldh, __half* __restrict__ H) {
+  const int64_t m = n * ldh;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / ldh;
+    const int c = (int)(t - r * ldh);
+    H[t] = c < dd ? __float2half_rn(X[r * dd + c]) : __float2half_rn(0.0f);
+  }
 }
 
 // d2 of each row to its k listed neighbours (FP32, full space), optionally sorted
@@ -237,11 +242,134 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
   }
 }
 
-// ---- one NNDescent iteration, one warp per row ------------------------------------
+// ---- distance phase helpers ------------------------------------------------------
+// FP16 rows (pitch a multiple of 8 halves, zero padded): 16 candidates per warp
+// step on the tensor cores.  mma.m16n8k16 multiplies A (16 candidate rows x 16
+// dims) by B (16 dims x 8 columns, every column the query row), FP32 accumulate.
+// Thread (g = lane / 4, c = lane % 4) supplies A for rows g and g + 8 and B for
+// column g at the logical k positions {2c, 2c+1, 2c+8, 2c+9}; it loads 16-byte
+// chunks c + 4s of the rows and of the query, and maps their halves 0-3 to one
+// mma and 4-7 to the next.  The k positions of A and B come from the same physical
+// dims (the map depends on c alone), so every column of D is the dot product.
+__device__ __forceinline__ void mma_f16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                        uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// d2 for the candidates todo[0, n_todo) of one row, FP16 space: cd[t] for each.
+// Two independent 16-candidate tiles per step keep four row loads in flight per
+// thread.
+__device__ __forceinline__ void dists_f16(const __half* __restrict__ X, int ldx, const __half* xs, const float* sqd,
+                                          float sqi, int64_t row, const int32_t* cid, const uint16_t* todo,
+                                          int n_todo, float* cd, int lane) {
+  const int V = ldx / 8;  // 16-byte chunks per row
+  const int S = (V + 3) / 4;
+  const int g = lane >> 2, c = lane & 3;
+  const uint4* xq = reinterpret_cast<const uint4*>(xs);
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int p0 = 0; p0 < n_todo; p0 += 32) {
+    int t[4], cc[4];
+    bool v[4];
+    const uint4* r[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {  // tile rows g, g + 8 (tile 0) and g + 16, g + 24 (tile 1)
+      const int p = p0 + g + 8 * u;
+      v[u] = p < n_todo;
+      t[u] = v[u] ? todo[p] : 0;
+      cc[u] = v[u] ? cid[t[u]] : (int)row;
+      r[u] = reinterpret_cast<const uint4*>(X + (int64_t)cc[u] * ldx);
+    }
+    float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+    for (int st = 0; st < S; ++st) {
+      const int q = c + 4 * st;
+      const bool in = q < V;
+      uint4 A[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) A[u] = (in && v[u]) ? __ldg(r[u] + q) : zero;
+      const uint4 B = in ? xq[q] : zero;
+      mma_f16(d0, A[0].x, A[1].x, A[0].y, A[1].y, B.x, B.y);
+      mma_f16(d0, A[0].z, A[1].z, A[0].w, A[1].w, B.z, B.w);
+      mma_f16(d1, A[2].x, A[3].x, A[2].y, A[3].y, B.x, B.y);
+      mma_f16(d1, A[2].z, A[3].z, A[2].w, A[3].w, B.z, B.w);
+    }
+    // d0[0]: row g, d0[2]: row g + 8, d1[0]: row g + 16, d1[2]: row g + 24 (every column
+    // holds the same dot); lane c stores row g + 8c
+    const float dot = c == 0 ? d0[0] : c == 1 ? d0[2] : c == 2 ? d1[0] : d1[2];
+    const int tt = c == 0 ? t[0] : c == 1 ? t[1] : c == 2 ? t[2] : t[3];
+    const int cs = c == 0 ? cc[0] : c == 1 ? cc[1] : c == 2 ? cc[2] : cc[3];
+    const bool vs = c == 0 ? v[0] : c == 1 ? v[1] : c == 2 ? v[2] : v[3];
+    if (vs) cd[tt] = d2_from_dot(sqi, sqd[cs], dot, true);
+  }
+}
+
+// FP32 rows: G lanes per candidate, each lane group working on two candidates at
+// once (2 * 32 / G per warp step), float4 loads when the pitch allows, a
+// log2(G)-step shuffle reduction.
+template <bool VEC>
+__device__ __forceinline__ void dists_f32(const float* __restrict__ X, int dd, int ldx, const float* xs,
+                                          const float* sqd, float sqi, int64_t row, const int32_t* cid,
+                                          const uint16_t* todo, int n_todo, float* cd, int lane, int G) {
+  const int C = 32 / G;
+  const int j = lane & (G - 1), slot = lane / G;
+  for (int p0 = 0; p0 < n_todo; p0 += 2 * C) {
+    const int pa = p0 + slot, pb = p0 + C + slot;
+    const bool va = pa < n_todo, vb = pb < n_todo;
+    const int ta = va ? todo[pa] : 0, tb = vb ? todo[pb] : 0;
+    const int ca = va ? cid[ta] : (int)row, cb = vb ? cid[tb] : (int)row;
+    float acc_a = 0.f, acc_b = 0.f;
+    if (VEC) {
+      const float4* ra = reinterpret_cast<const float4*>(X + (int64_t)ca * ldx);
+      const float4* rb = reinterpret_cast<const float4*>(X + (int64_t)cb * ldx);
+      const float4* xp = reinterpret_cast<const float4*>(xs);
+      const int V = dd / 4;
+#pragma unroll 4
+      for (int q = j; q < V; q += G) {
+        const float4 x = xp[q];
+        const float4 a4 = __ldg(ra + q);
+        const float4 b4 = vb ? __ldg(rb + q) : make_float4(0.f, 0.f, 0.f, 0.f);
+        acc_a = fmaf(x.x, a4.x, acc_a);
+        acc_a = fmaf(x.y, a4.y, acc_a);
+        acc_a = fmaf(x.z, a4.z, acc_a);
+        acc_a = fmaf(x.w, a4.w, acc_a);
+        acc_b = fmaf(x.x, b4.x, acc_b);
+        acc_b = fmaf(x.y, b4.y, acc_b);
+        acc_b = fmaf(x.z, b4.z, acc_b);
+        acc_b = fmaf(x.w, b4.w, acc_b);
+      }
+    } else {
+      const float* ra = X + (int64_t)ca * ldx;
+      const float* rb = X + (int64_t)cb * ldx;
+      for (int q = j; q < dd; q += G) {
+        const float x = xs[q];
+        acc_a = fmaf(x, __ldg(ra + q), acc_a);
+        if (vb) acc_b = fmaf(x, __ldg(rb + q), acc_b);
+      }
+    }
+    for (int o = G >> 1; o > 0; o >>= 1) {
+      acc_a += __shfl_xor_sync(0xffffffffu, acc_a, o);
+      acc_b += __shfl_xor_sync(0xffffffffu, acc_b, o);
+    }
+    if (va && j == 0) cd[ta] = d2_from_dot(sqi, sqd[ca], acc_a, false);
+    if (vb && j == 1 % G) cd[tb] = d2_from_dot(sqi, sqd[cb], acc_b, false);
+  }
+}
+
+// dedup hash (4 hcap bytes), later candidate distances (4 tcap) + to-do list (2 tcap)
+__host__ __device__ inline size_t iter_scratch_bytes(int tcap, int hcap) {
+  const size_t a = (size_t)hcap * 4, b = (size_t)tcap * 6;
+  return ((a > b ? a : b) + 15) / 16 * 16;
+}
+
 struct IterArgs {
-  const void* Xd;  // distance space, float or __half rows of length dd
+  const void* Xd;  // distance space, float or __half rows of length dd, pitch ldx elements
   const float* sqd;
-  int dd;
+  int dd, ldx;
+  int group;  // FP32 rows: lanes per candidate (4, 8, 16 or 32)
   const int32_t* idx_old;
   const float* dist_old;
   const uint8_t* flags_old;  // converging path only
@@ -249,7 +377,7 @@ struct IterArgs {
   int64_t n;
   int k, mc_new, j_nn;
   int converging, recompute_cur, half_round;
-  int tcap, hcap;  // candidate capacity per row (multiple of 32) and hash size (power of two)
+  int tcap, hcap, hbits;  // candidate capacity per row (multiple of 32); hash size 2^hbits
   int32_t* idx_new;
   float* dist_new;
   uint8_t* flags_new;
@@ -258,18 +386,23 @@ struct IterArgs {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
-  const size_t per_warp = (size_t)a.dd * sizeof(T) + (size_t)a.tcap * 12 + (size_t)a.hcap * 4 + 32 * 4;
-  uint8_t* base = smem_raw + warp * ((per_warp + 15) / 16 * 16);
+  // per warp: query row | candidate ids | scratch (the dedup hash table, then the
+  // candidate distances and the to-do list) | sources
+  const size_t xs_bytes = ((size_t)a.ldx * sizeof(T) + 15) / 16 * 16;
+  const size_t scratch = iter_scratch_bytes(a.tcap, a.hcap);
+  const size_t per_warp = xs_bytes + (size_t)a.tcap * 4 + scratch + 32 * 4;
+  uint8_t* base = smem_raw + warp * per_warp;
   T* xs = reinterpret_cast<T*>(base);
-  int32_t* cid = reinterpret_cast<int32_t*>(base + (a.dd * sizeof(T) + 15) / 16 * 16);
-  float* cd = reinterpret_cast<float*>(cid + a.tcap);
-  int32_t* todo = reinterpret_cast<int32_t*>(cd + a.tcap);
-  int32_t* htab = todo + a.tcap;
-  int32_t* srcs = htab + a.hcap;
+  int32_t* cid = reinterpret_cast<int32_t*>(base + xs_bytes);
+  uint8_t* scr = reinterpret_cast<uint8_t*>(cid + a.tcap);
+  int32_t* htab = reinterpret_cast<int32_t*>(scr);
+  float* cd = reinterpret_cast<float*>(scr);
+  uint16_t* todo = reinterpret_cast<uint16_t*>(cd + a.tcap);
+  int32_t* srcs = reinterpret_cast<int32_t*>(scr + scratch);
   if (row >= a.n) return;
   const int k = a.k;
   const int32_t* orow = a.idx_old + row * k;
@@ -297,7 +430,7 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
   } else {
     if (lane < k) srcs[lane] = my_old;
   }
-  for (int t = lane; t < a.dd; t += 32) xs[t] = reinterpret_cast<const T*>(a.Xd)[row * a.dd + t];
+  for (int t = lane; t < a.ldx; t += 32) xs[t] = reinterpret_cast<const T*>(a.Xd)[row * a.ldx + t];
   for (int t = lane; t < a.hcap; t += 32) htab[t] = -1;
   __syncwarp();
 
@@ -319,16 +452,17 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
   }
   __syncwarp();
 
-  // 2. first-occurrence dedup + 3. list of distances to compute
-  int n_todo = 0;
-  for (int t0 = 0; t0 < a.tcap; t0 += 32) {
+  // 2. first-occurrence dedup (bit c of `keep`: this lane's column in chunk c is the
+  // first occurrence of its id and not the row itself)
+  unsigned long long keep = 0ull;
+  for (int t0 = 0, ch = 0; t0 < a.tcap; t0 += 32, ++ch) {
     const int t = t0 + lane;
     const int id = cid[t];
     const bool valid = t < T_total;
     const unsigned same = __match_any_sync(0xffffffffu, id);
     bool first = valid && (__ffs(same) - 1) == lane;  // lowest lane of an equal-id group in this chunk
     if (first) {
-      unsigned h = ((unsigned)id * 0x9E3779B1u) & (unsigned)(a.hcap - 1);
+      unsigned h = ((unsigned)id * 0x9E3779B1u) >> (32 - a.hbits);
       while (true) {
         const int old = atomicCAS(&htab[h], -1, id);
         if (old == -1) break;
@@ -339,40 +473,36 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
         h = (h + 1) & (unsigned)(a.hcap - 1);
       }
     }
+    if (first && id != (int)row) keep |= 1ull << ch;
+  }
+  __syncwarp();  // the hash table is dead; its space becomes cd / todo
+
+  // 3. stored distances and the list of distances to compute
+  int n_todo = 0;
+  for (int t0 = 0, ch = 0; t0 < a.tcap; t0 += 32, ++ch) {
+    const int t = t0 + lane;
     float d = kBig;
     bool need = false;
-    if (first && id != (int)row) {
+    if ((keep >> ch) & 1ull) {
       if (t < k && !a.recompute_cur) d = a.dist_old[row * k + t];
       else need = true;
     }
     cd[t] = d;
     const unsigned nb = __ballot_sync(0xffffffffu, need);
-    if (need) todo[n_todo + __popc(nb & ((1u << lane) - 1u))] = t;
+    if (need) todo[n_todo + __popc(nb & ((1u << lane) - 1u))] = (uint16_t)t;
     n_todo += __popc(nb);
   }
   __syncwarp();
   const float sqi = a.sqd[row];
-  for (int p0 = 0; p0 < n_todo; p0 += 4) {
-    int c[4], tt[4];
-    const int cnt = min(4, n_todo - p0);
-    for (int u = 0; u < 4; ++u) {
-      tt[u] = u < cnt ? todo[p0 + u] : 0;
-      c[u] = u < cnt ? cid[tt[u]] : 0;
-    }
-    float dots[4];
-    dot4<T>(reinterpret_cast<const T*>(a.Xd), xs, a.dd, c, cnt, lane, dots);
-    if (lane < cnt) {
-      float dot = dots[0];
-      int my_t = tt[0], my_c = c[0];
-#pragma unroll
-      for (int u = 1; u < 4; ++u)
-        if (lane == u) {
-          dot = dots[u];
-          my_t = tt[u];
-          my_c = c[u];
-        }
-      cd[my_t] = d2_from_dot(sqi, a.sqd[my_c], dot, a.half_round != 0);
-    }
+  if constexpr (sizeof(T) == 2) {
+    dists_f16(reinterpret_cast<const __half*>(a.Xd), a.ldx, reinterpret_cast<const __half*>(xs), a.sqd, sqi, row,
+              cid, todo, n_todo, cd, lane);
+  } else if ((a.ldx & 3) == 0 && (a.dd & 3) == 0) {
+    dists_f32<true>(reinterpret_cast<const float*>(a.Xd), a.dd, a.ldx, reinterpret_cast<const float*>(xs), a.sqd,
+                    sqi, row, cid, todo, n_todo, cd, lane, a.group);
+  } else {
+    dists_f32<false>(reinterpret_cast<const float*>(a.Xd), a.dd, a.ldx, reinterpret_cast<const float*>(xs), a.sqd,
+                     sqi, row, cid, todo, n_todo, cd, lane, a.group);
   }
   __syncwarp();
 
@@ -413,9 +543,8 @@ __global__ void __launch_bounds__(kWarps * 32) iter_kernel(IterArgs a) {
 
 using namespace umapb;
 
-static size_t iter_smem_per_warp(int dd, int elem, int tcap, int hcap) {
-  const size_t per_warp = (size_t)dd * elem + (size_t)tcap * 12 + (size_t)hcap * 4 + 32 * 4 + 16;
-  return (per_warp + 15) / 16 * 16;
+static size_t iter_smem_per_warp(int ldx, int elem, int tcap, int hcap) {
+  return ((size_t)ldx * elem + 15) / 16 * 16 + (size_t)tcap * 4 + nnd::iter_scratch_bytes(tcap, hcap) + 32 * 4;
 }
 
 namespace umapb {
@@ -454,13 +583,15 @@ extern "C" int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t h
   return UMAPB_OK;
 }
 
-extern "C" int umapb_nnd_to_half(const float* X, int64_t count, void* H, umapb_stream_t stream_) {
+extern "C" int umapb_nnd_to_half(const float* X, int64_t n, int32_t dd, int32_t ldh, void* H,
+                                 umapb_stream_t stream_) {
   clear_error();
-  UMAPB_REQUIRE(X && H && count >= 0, "nnd_to_half: bad arguments");
+  UMAPB_REQUIRE(X && H && n >= 0 && dd >= 1 && ldh >= dd, "nnd_to_half: bad arguments");
+  const int64_t count = n * ldh;
   if (count == 0) return UMAPB_OK;
   const int64_t want = ceil_div(count, 256);
   const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
-  nnd::to_half_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(X, count,
+  nnd::to_half_kernel<<<blocks, 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(X, n, dd, ldh,
                                                                                     static_cast<__half*>(H));
   UMAPB_LAUNCH_CHECK("nnd_to_half kernel");
   count_launches(1);
@@ -534,7 +665,8 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   return UMAPB_OK;
 }
 
-extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t half, const int32_t* idx_old,
+extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
+                                   const int32_t* idx_old,
                                    const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n,
                                    int32_t k, int32_t mc_new, int32_t j_nn, int32_t converging,
                                    int32_t recompute_cur, int32_t* idx_new, float* dist_new, uint8_t* flags_new,
@@ -545,13 +677,22 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   UMAPB_REQUIRE(Xd && sqd && idx_old && dist_old && idx_new && dist_new && flags_new && changed,
                 "nnd_iteration: null array argument");
   UMAPB_REQUIRE(!converging || flags_old, "nnd_iteration: the converging path needs the flags");
-  UMAPB_REQUIRE(n >= 2 && dd >= 1, "nnd_iteration: bad shape");
+  UMAPB_REQUIRE(n >= 2 && dd >= 1 && ldx >= dd, "nnd_iteration: bad shape");
+  UMAPB_REQUIRE(!half || (ldx % 8 == 0 && (reinterpret_cast<uintptr_t>(Xd) & 15) == 0),
+                "nnd_iteration: FP16 rows need a pitch that is a multiple of 8 and a 16-byte aligned base");
+  UMAPB_REQUIRE(half || ldx % 4 != 0 || dd % 4 != 0 || (reinterpret_cast<uintptr_t>(Xd) & 15) == 0,
+                "nnd_iteration: FP32 rows need a 16-byte aligned base");
   UMAPB_REQUIRE(k >= 1 && k <= 32, "nnd_iteration: k must be in [1, 32]");
   UMAPB_REQUIRE(mc_new >= 0 && mc_new <= k && j_nn >= 0 && j_nn <= k, "nnd_iteration: bad mc_new / j_nn");
   nnd::IterArgs a;
   a.Xd = Xd;
   a.sqd = sqd;
   a.dd = dd;
+  a.ldx = ldx;
+  {
+    const int V = half ? ldx / 8 : (ldx + 3) / 4;  // 16-byte chunks per row
+    a.group = V <= 32 ? 4 : V <= 128 ? 8 : 16;
+  }
   a.idx_old = idx_old;
   a.dist_old = dist_old;
   a.flags_old = flags_old;
@@ -565,15 +706,19 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.half_round = half;
   const int T = k + mc_new * j_nn + (rev ? k : 0);
   a.tcap = (T + 31) / 32 * 32;
-  int h = 64;
-  while (h < 2 * T) h <<= 1;
+  int h = 64, hb = 6;
+  while (h < 2 * T) {
+    h <<= 1;
+    ++hb;
+  }
   a.hcap = h;
+  a.hbits = hb;
   a.idx_new = idx_new;
   a.dist_new = dist_new;
   a.flags_new = flags_new;
   a.changed = changed;
   a.evals = evals;
-  const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(dd, half ? 2 : 4, a.tcap, a.hcap);
+  const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(ldx, half ? 2 : 4, a.tcap, a.hcap);
   UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_iteration: row dimension too large for shared memory");
   static bool attr = false;
   if (!attr) {

@@ -77,15 +77,23 @@ __device__ __forceinline__ double unit53(uint32_t a, uint32_t b) {
   return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
 }
 
+// Where normal number g goes.  Projections (affine == 0): g < g1 into P, the rest
+// into P2, as float32(float32(g) / s).  Affine (affine != 0): float32(loc + scale g)
+// into P (RandomState.normal(loc, scale) cast to float32).
 struct Out {
+  int affine;
   int64_t g1;  // normals for P (d * 100, or 0)
   float* P;
-  double s1;   // sqrt(100) as NumPy computes it
+  double s1;   // sqrt(100) as NumPy computes it; loc when affine
   float* P2;
-  double s2;
+  double s2;   // sqrt(300); scale when affine
 };
 
 __device__ __forceinline__ void emit(const Out& o, int64_t g, double v) {
+  if (o.affine) {
+    o.P[g] = __double2float_rn(__dadd_rn(o.s1, __dmul_rn(o.s2, v)));
+    return;
+  }
   const double x = (double)__double2float_rn(v);
   if (g < o.g1)
     o.P[g] = __double2float_rn(__ddiv_rn(x, o.s1));
@@ -239,6 +247,7 @@ extern "C" int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int
   uint32_t mask = rng;
   for (int s = 1; s <= 16; s <<= 1) mask |= mask >> s;
   rstart::Out out;
+  out.affine = 0;
   out.g1 = (int64_t)d * pd1;
   out.P = P;
   out.s1 = sqrt((double)(pd1 > 0 ? pd1 : 1));
@@ -248,6 +257,26 @@ extern "C" int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int
   rstart::random_start_kernel<<<1, rstart::kThreads, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
       state, k, n * (int64_t)k, rng, mask, idx, G, out);
   UMAPB_LAUNCH_CHECK("nnd_random_start kernel");
+  count_launches(1);
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out,
+                                   umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(state && (out || count == 0) && count >= 0, "legacy_normal: bad arguments");
+  if (count == 0) return UMAPB_OK;
+  rstart::Out o;
+  o.affine = 1;
+  o.g1 = count;
+  o.P = out;
+  o.s1 = loc;
+  o.P2 = nullptr;
+  o.s2 = scale;
+  // no bounded integers (count 0): the kernel goes straight to the normals
+  rstart::random_start_kernel<<<1, rstart::kThreads, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
+      state, 1, 0, 1u, 1u, nullptr, count, o);
+  UMAPB_LAUNCH_CHECK("legacy_normal kernel");
   count_launches(1);
   return UMAPB_OK;
 }

@@ -63,3 +63,14 @@ def test_workspace_queries_and_argument_errors(lib):
     with pytest.raises(_lib.UmapB200Error):
         _lib.query("umapb_spectral_workspace", 100, 7, 1000, 100)
     assert _lib.load().umapb_abi_version() == 1
+
+
+def test_python_signatures_have_the_header_arity():
+    """Each ctypes argument list has as many entries as the C declaration has parameters."""
+    from mlx_vis_b200 import _lib
+
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    for name, params in re.findall(r"\b(umapb_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text):
+        params = params.strip()
+        n = 0 if params in ("", "void") else params.count(",") + 1
+        assert len(_lib.SIGNATURES[name]) == n, (name, n, len(_lib.SIGNATURES[name]))
