@@ -119,6 +119,10 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     shifted past the row index, then P (d, pd1) and P2 (d, pd2) =
  *                     float32(float32(randn) / sqrt(pd)) for pd > 0 (0 skips the
  *                     draw); `state` is overwritten with the state after the draws.
+ *                     With a workspace (size from the _workspace query) the draws
+ *                     run grid-wide on words generated ahead with a 10-sigma
+ *                     margin (a shortfall is redone on the device by one CTA);
+ *                     without one, one CTA walks the stream.
  * ------------------------------------------------------------------------- */
 int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq, umapb_stream_t stream);
 int umapb_nnd_to_half(const float* X, int64_t n, int32_t dd, int32_t ldh, void* H, umapb_stream_t stream);
@@ -133,14 +137,18 @@ int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ld
                         float* dist_new, uint8_t* flags_new, unsigned long long* changed,
                         unsigned long long* evals, umapb_stream_t stream);
 int umapb_nnd_sqrt(const float* d2, int64_t count, float* out, umapb_stream_t stream);
+int umapb_nnd_random_start_workspace(int64_t n, int32_t k, int32_t d, int32_t pd1, int32_t pd2, size_t* bytes);
 int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P, int32_t pd1,
-                           float* P2, int32_t pd2, umapb_stream_t stream);
+                           float* P2, int32_t pd2, void* workspace, size_t workspace_bytes,
+                           umapb_stream_t stream);
 /* umapb_legacy_normal: count values float32(loc + scale * g) with g NumPy's legacy
  * standard normals drawn from `state` (same buffer layout as above; overwritten
  * with the state after the draws) — RandomState(seed).normal(loc, scale, count)
- * cast to float32, as the spectral init's noise (umap.py:344-346). */
-int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out,
-                        umapb_stream_t stream);
+ * cast to float32, as the spectral init's noise (umap.py:344-346).  Workspace as
+ * for umapb_nnd_random_start. */
+int umapb_legacy_normal_workspace(int64_t count, size_t* bytes);
+int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out, void* workspace,
+                        size_t workspace_bytes, umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Fuzzy simplicial set — replaces UMAP._fuzzy_simplicial_set

@@ -55,8 +55,10 @@ SIGNATURES = {
     "umapb_mlp_rowsum": [_p, _i32, _i32, _i32, _p, _p],
     "umapb_adamw": [_p, _p, _p, _p, _i32, _i32, _f32, _f32, _f32, _f32, _f32, _i32, _p, _i32, _p, _i32, _p],
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
-    "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p],
-    "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p],
+    "umapb_nnd_random_start_workspace": [_i64, _i32, _i32, _i32, _i32, _psz],
+    "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p, _sz, _p],
+    "umapb_legacy_normal_workspace": [_i64, _psz],
+    "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p, _sz, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],
@@ -196,14 +198,17 @@ def normal(shape, seed: int, device) -> torch.Tensor:
     return out
 
 
-def legacy_normal(rs, shape, loc: float, scale: float, device) -> torch.Tensor:
+def legacy_normal(rs, shape, loc: float, scale: float, device, parallel: bool = True) -> torch.Tensor:
     """float32(rs.normal(loc, scale, shape)) for a NumPy RandomState ``rs``, drawn on
-    the device from rs's state (umapb_legacy_normal); ``rs`` itself is not advanced."""
+    the device from rs's state (umapb_legacy_normal); ``rs`` itself is not advanced.
+    ``parallel=False`` takes the one-CTA walk instead of the grid-wide path."""
     from mlx_vis_b200._nndescent.nndescent import state_words
 
     state = torch.from_numpy(state_words(rs.get_state())).to(device)
     out = torch.empty(shape, dtype=torch.float32, device=device)
-    call("umapb_legacy_normal", ptr(state), out.numel(), float(loc), float(scale), ptr(out), stream_handle())
+    ws = workspace(query("umapb_legacy_normal_workspace", out.numel()), device) if parallel else None
+    call("umapb_legacy_normal", ptr(state), out.numel(), float(loc), float(scale), ptr(out), ptr(ws),
+         ws.numel() if ws is not None else 0, stream_handle())
     return out
 
 

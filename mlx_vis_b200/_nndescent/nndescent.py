@@ -65,22 +65,25 @@ def words_state(w: np.ndarray):
     return ("MT19937", w[:624].copy(), int(w[624]), int(w[625]), float(w[626:628].view(np.float64)[0]))
 
 
-def random_start_device(n: int, k: int, d: int, random_state, dev):
+def random_start_device(n: int, k: int, d: int, random_state, dev, parallel: bool = True):
     """The reference's draws made on the device (umapb_nnd_random_start).
 
     Seeds NumPy's global stream like the reference, hands its state to the
-    kernel and returns (idx, P, P2, state) with ``state`` the device buffer that
+    kernels and returns (idx, P, P2, state) with ``state`` the device buffer that
     holds the stream's state after the draws (give it back with
-    ``np.random.set_state(words_state(state.cpu().numpy()))``)."""
+    ``np.random.set_state(words_state(state.cpu().numpy()))``).  ``parallel=False``
+    takes the one-CTA walk instead of the grid-wide path."""
     if random_state is not None:
         np.random.seed(random_state)
     state = torch.from_numpy(state_words(np.random.get_state())).to(dev)
     pd1, pd2 = min(100, d), min(300, d)
+    pd1, pd2 = (pd1 if pd1 < d else 0), (pd2 if pd2 < d else 0)
     idx = torch.empty((n, k), dtype=torch.int32, device=dev)
-    P = torch.empty((d, pd1), dtype=torch.float32, device=dev) if pd1 < d else None
-    P2 = torch.empty((d, pd2), dtype=torch.float32, device=dev) if pd2 < d else None
-    call("umapb_nnd_random_start", ptr(state), n, k, d, ptr(idx), ptr(P), pd1 if P is not None else 0, ptr(P2),
-         pd2 if P2 is not None else 0, stream_handle())
+    P = torch.empty((d, pd1), dtype=torch.float32, device=dev) if pd1 else None
+    P2 = torch.empty((d, pd2), dtype=torch.float32, device=dev) if pd2 else None
+    ws = _lib.workspace(query("umapb_nnd_random_start_workspace", n, k, d, pd1, pd2), dev) if parallel else None
+    call("umapb_nnd_random_start", ptr(state), n, k, d, ptr(idx), ptr(P), pd1, ptr(P2), pd2, ptr(ws),
+         ws.numel() if ws is not None else 0, stream_handle())
     return idx, P, P2, state
 
 

@@ -8,17 +8,27 @@
 // Those are MT19937 words (Matsumoto & Nishimura 1998) turned into bounded
 // integers by masked rejection and into normals by Marsaglia's polar method on
 // 53-bit doubles.  Every output depends on how many words the rejections before
-// it consumed, so the stream is walked by one CTA: 640 threads hold one state
-// word each, a generation (twist) takes three dependent phases, and each
-// generation's 624 words are tested, ranked with a block scan and scattered to
-// their output slots in parallel.  The state enters and leaves in NumPy's
-// get_state() layout, so the host hands the stream back to NumPy afterwards.
+// it consumed.
+//
+// Parallel path (with a workspace): one CTA only runs the MT recurrence and
+// stores the raw state of every generation, enough words for the requested
+// counts with a 10-sigma margin on the rejections; the acceptance tests, ranks
+// (block counts + scan) and output scatter then run over the whole grid, first
+// for the integers, then for the normal pairs starting at the word where the
+// integers stopped.  A final kernel rebuilds NumPy's state at the word where the
+// draws stopped.  If the margin ever falls short (a status word in the
+// workspace), a gated one-CTA walk, launched behind them and otherwise exiting at
+// once, redoes all the draws from a copy of the incoming state.
+// Sequential path (no workspace): the same one-CTA walk, generation by
+// generation, testing and ranking each generation's 624 words in parallel.
 //
 // State buffer (uint32 words): key[624], pos, has_gauss, gauss (double, low word
-// first).  No waits: the loops end when the requested counts are produced.
+// first), NumPy's get_state() layout.  No waits: every loop ends when the
+// requested counts are produced or the generated words run out.
 #include <math.h>
 
 #include "common.cuh"
+#include "scan.cuh"
 
 namespace umapb {
 namespace rstart {
@@ -44,13 +54,12 @@ __device__ __forceinline__ uint32_t temper(uint32_t y) {
 // reads the NEW entry i + M - N once i >= N - M, and the last entry reads the new
 // entry 0: three phases of 227, 227 and 170 entries.
 __device__ __forceinline__ void twist(const uint32_t* __restrict__ o, uint32_t* __restrict__ w) {
-  const int t = threadIdx.x;
-  if (t < kHalf) w[t] = o[t + kM] ^ mix(o[t], o[t + 1]);
+  for (int i = threadIdx.x; i < kHalf; i += blockDim.x) w[i] = o[i + kM] ^ mix(o[i], o[i + 1]);
   __syncthreads();
-  if (t >= kHalf && t < 2 * kHalf) w[t] = w[t - kHalf] ^ mix(o[t], o[t + 1]);
+  for (int i = kHalf + threadIdx.x; i < 2 * kHalf; i += blockDim.x) w[i] = w[i - kHalf] ^ mix(o[i], o[i + 1]);
   __syncthreads();
-  if (t >= 2 * kHalf && t < kN - 1) w[t] = w[t - kHalf] ^ mix(o[t], o[t + 1]);
-  if (t == kN - 1) w[t] = w[kM - 1] ^ mix(o[kN - 1], w[0]);
+  for (int i = 2 * kHalf + threadIdx.x; i < kN - 1; i += blockDim.x) w[i] = w[i - kHalf] ^ mix(o[i], o[i + 1]);
+  if (threadIdx.x == 0) w[kN - 1] = w[kM - 1] ^ mix(o[kN - 1], w[0]);
   __syncthreads();
 }
 
@@ -101,19 +110,23 @@ __device__ __forceinline__ void emit(const Out& o, int64_t g, double v) {
     o.P2[g - o.g1] = __double2float_rn(__ddiv_rn(x, o.s2));
 }
 
-__global__ void __launch_bounds__(kThreads) random_start_kernel(uint32_t* __restrict__ state, int k, int64_t count,
-                                                                uint32_t rng, uint32_t mask,
-                                                                int32_t* __restrict__ idx, int64_t G, Out out) {
+// One CTA walks the stream from in_state and leaves the final state in state.
+// With a gate, it runs only when *gate != 0 (the grid-wide path fell short).
+__global__ void __launch_bounds__(kThreads) walk_kernel(const uint32_t* __restrict__ in_state,
+                                                        uint32_t* __restrict__ state, const int32_t* __restrict__ gate,
+                                                        int k, int64_t count, uint32_t rng, uint32_t mask,
+                                                        int32_t* __restrict__ idx, int64_t G, Out out) {
+  if (gate && *gate == 0) return;
   __shared__ uint32_t key[2][kN];
   __shared__ uint32_t words[kN + 4];
   __shared__ int warp_sum[kThreads / 32];
   __shared__ int s_pos, s_has;
   __shared__ double s_gauss;
   const int t = threadIdx.x;
-  for (int i = t; i < kN; i += kThreads) key[0][i] = state[i];
-  int pos = (int)state[kN];
-  int has_gauss = (int)state[kN + 1];
-  double gauss = __hiloint2double((int)state[kN + 3], (int)state[kN + 2]);
+  for (int i = t; i < kN; i += kThreads) key[0][i] = in_state[i];
+  int pos = (int)in_state[kN];
+  int has_gauss = (int)in_state[kN + 1];
+  double gauss = __hiloint2double((int)in_state[kN + 3], (int)in_state[kN + 2]);
   int cur = 0;
   __syncthreads();
 
@@ -231,21 +244,304 @@ __global__ void __launch_bounds__(kThreads) random_start_kernel(uint32_t* __rest
   }
 }
 
+
+// ---- parallel path -------------------------------------------------------------
+constexpr int kPar = 256;          // threads per block
+constexpr int kIntPerBlock = 1024;  // stream words per block (4 per thread)
+constexpr int kAttPerBlock = 512;   // normal attempts per block (2 per thread)
+
+struct Scalars {
+  int64_t tot_int, tot_att;  // accepted integers / attempts in the generated words
+  int64_t int_stop;          // stream words the integers consumed
+  int64_t end;               // stream words consumed after the normals
+  double gauss_out;
+  int32_t has_out;
+  int32_t status;  // nonzero: the generated words fell short; the gated walk redoes the draws
+};
+
+// raw[624 g + i] = word i of generation g (generation 0 = the incoming key)
+__global__ void __launch_bounds__(kPar) stream_kernel(const uint32_t* __restrict__ state, int64_t n_gen,
+                                                      uint32_t* __restrict__ raw) {
+  __shared__ uint32_t key[2][kN];
+  for (int i = threadIdx.x; i < kN; i += kPar) {
+    key[0][i] = state[i];
+    raw[i] = state[i];
+  }
+  __syncthreads();
+  int cur = 0;
+  for (int64_t g = 1; g <= n_gen; ++g) {
+    twist(key[cur], key[cur ^ 1]);
+    cur ^= 1;
+    for (int i = threadIdx.x; i < kN; i += kPar) raw[g * kN + i] = key[cur][i];
+  }
+}
+
+// exclusive prefix of v over the block (kPar threads) and the block total
+__device__ __forceinline__ int block_excl(int v, int* warp_tot, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  int before = 0;
+  total = 0;
+#pragma unroll
+  for (int w = 0; w < kPar / 32; ++w) {
+    const int c = warp_tot[w];
+    before += w < warp ? c : 0;
+    total += c;
+  }
+  __syncthreads();
+  return before + x - v;
+}
+
+__device__ __forceinline__ uint32_t word_at(const uint32_t* raw, const uint32_t* state, int64_t w) {
+  return temper(raw[(int64_t)state[kN] + w]);
+}
+
+__global__ void __launch_bounds__(kPar) int_count_kernel(const uint32_t* __restrict__ raw,
+                                                         const uint32_t* __restrict__ state, int64_t Wi,
+                                                         uint32_t rng, uint32_t mask, int32_t* __restrict__ counts) {
+  __shared__ int warp_tot[kPar / 32];
+  const int64_t w0 = (int64_t)blockIdx.x * kIntPerBlock + 4 * threadIdx.x;
+  int c = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+    if (w0 + u < Wi) c += (word_at(raw, state, w0 + u) & mask) <= rng ? 1 : 0;
+  int total;
+  block_excl(c, warp_tot, total);
+  if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kPar) int_scatter_kernel(const uint32_t* __restrict__ raw,
+                                                           const uint32_t* __restrict__ state, int64_t Wi,
+                                                           uint32_t rng, uint32_t mask,
+                                                           const int32_t* __restrict__ offsets, int64_t count, int k,
+                                                           int32_t* __restrict__ idx, Scalars* sc) {
+  __shared__ int warp_tot[kPar / 32];
+  const int64_t w0 = (int64_t)blockIdx.x * kIntPerBlock + 4 * threadIdx.x;
+  uint32_t v[4];
+  bool acc[4];
+  int c = 0;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    v[u] = w0 + u < Wi ? word_at(raw, state, w0 + u) & mask : 0xffffffffu;
+    acc[u] = w0 + u < Wi && v[u] <= rng;
+    c += acc[u] ? 1 : 0;
+  }
+  int total;
+  int64_t r = offsets[blockIdx.x] + block_excl(c, warp_tot, total);
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    if (!acc[u]) continue;
+    if (r < count) idx[r] = (int32_t)((int64_t)v[u] >= r / k ? v[u] + 1u : v[u]);
+    if (r == count - 1) sc->int_stop = w0 + u + 1;
+    ++r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && sc->tot_int < count) atomicOr(&sc->status, 1);
+}
+
+// attempt a of the normals uses stream words int_stop + 4a .. + 3
+__device__ __forceinline__ bool attempt(const uint32_t* raw, const uint32_t* state, int64_t w, double& x1,
+                                        double& x2, double& r2) {
+  x1 = 2.0 * unit53(word_at(raw, state, w), word_at(raw, state, w + 1)) - 1.0;
+  x2 = 2.0 * unit53(word_at(raw, state, w + 2), word_at(raw, state, w + 3)) - 1.0;
+  r2 = __dadd_rn(__dmul_rn(x1, x1), __dmul_rn(x2, x2));
+  return r2 < 1.0 && r2 != 0.0;
+}
+
+__global__ void __launch_bounds__(kPar) att_count_kernel(const uint32_t* __restrict__ raw,
+                                                         const uint32_t* __restrict__ state, const Scalars* sc,
+                                                         int64_t Aw, int32_t* __restrict__ counts) {
+  __shared__ int warp_tot[kPar / 32];
+  const int64_t a0 = (int64_t)blockIdx.x * kAttPerBlock + 2 * threadIdx.x;
+  const int64_t s = sc->int_stop;
+  int c = 0;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    double x1, x2, r2;
+    if (a0 + u < Aw) c += attempt(raw, state, s + 4 * (a0 + u), x1, x2, r2) ? 1 : 0;
+  }
+  int total;
+  block_excl(c, warp_tot, total);
+  if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kPar) att_scatter_kernel(const uint32_t* __restrict__ raw,
+                                                           const uint32_t* __restrict__ state, Scalars* sc, int64_t Aw,
+                                                           const int32_t* __restrict__ offsets, int64_t G, Out out) {
+  __shared__ int warp_tot[kPar / 32];
+  const int64_t a0 = (int64_t)blockIdx.x * kAttPerBlock + 2 * threadIdx.x;
+  const int64_t s = sc->int_stop;
+  const int made0 = state[kN + 1] ? 1 : 0;  // a cached normal is used first
+  const int64_t pairs = (G - made0 + 1) / 2;
+  double x1[2], x2[2], r2[2];
+  bool acc[2];
+  int c = 0;
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    acc[u] = a0 + u < Aw && attempt(raw, state, s + 4 * (a0 + u), x1[u], x2[u], r2[u]);
+    c += acc[u] ? 1 : 0;
+  }
+  int total;
+  int64_t r = offsets[blockIdx.x] + block_excl(c, warp_tot, total);
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    if (!acc[u]) continue;
+    if (r < pairs) {
+      const double f = __dsqrt_rn(__ddiv_rn(-2.0 * log(r2[u]), r2[u]));
+      const int64_t g = made0 + 2 * r;
+      emit(out, g, __dmul_rn(f, x2[u]));
+      if (g + 1 < G) {
+        emit(out, g + 1, __dmul_rn(f, x1[u]));
+      } else {
+        sc->has_out = 1;
+        sc->gauss_out = __dmul_rn(f, x1[u]);
+      }
+    }
+    if (r == pairs - 1) sc->end = s + 4 * (a0 + u) + 4;
+    ++r;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (made0) emit(out, 0, __hiloint2double((int)state[kN + 3], (int)state[kN + 2]));
+    if (sc->tot_att < pairs) atomicOr(&sc->status, 2);
+  }
+}
+
+// NumPy's state after `consumed` stream words (and the normals' cache)
+__global__ void __launch_bounds__(kPar) final_state_kernel(const uint32_t* __restrict__ raw,
+                                                           uint32_t* __restrict__ state, const Scalars* sc,
+                                                           int64_t G) {
+  const int64_t pos0 = state[kN];
+  const int made0 = state[kN + 1] ? 1 : 0;
+  const int64_t pairs = G > 0 ? (G - made0 + 1) / 2 : 0;
+  const int64_t consumed = pairs > 0 ? sc->end : sc->int_stop;
+  __syncthreads();  // every thread has read the incoming state
+  if (consumed > 0) {
+    const int64_t e = pos0 + consumed;  // raw index after the last consumed word
+    const int64_t gen = (e - 1) / kN;
+    for (int i = threadIdx.x; i < kN; i += kPar) state[i] = raw[gen * kN + i];
+    if (threadIdx.x == 0) state[kN] = (uint32_t)(e - gen * kN);
+  }
+  if (threadIdx.x == 0 && G > 0) {
+    const int has = pairs > 0 ? sc->has_out : 0;
+    const double gs = pairs > 0 && has ? sc->gauss_out : 0.0;
+    state[kN + 1] = (uint32_t)has;
+    state[kN + 2] = (uint32_t)__double2loint(gs);
+    state[kN + 3] = (uint32_t)__double2hiint(gs);
+  }
+}
+
+__global__ void const_ints_kernel(int64_t count, int k, int32_t* __restrict__ idx) {
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < count; q += (int64_t)gridDim.x * blockDim.x)
+    idx[q] = (q / k) == 0 ? 1 : 0;
+}
+
+struct Plan {
+  int64_t Wi, Aw, n_gen, nbI, nbA;
+  size_t bytes;
+  Scalars* sc;
+  uint32_t* backup;  // the incoming state, for the gated walk
+  uint32_t* raw;
+  int32_t* cnt_i;
+  int32_t* cnt_a;
+};
+
+// Words for `count` integers accepted with probability p = (rng + 1) / (mask + 1)
+// and for the normal pairs (probability pi / 4), each with a 10-sigma margin.
+static Plan plan(void* ws, int64_t count, uint32_t rng, uint32_t mask, int64_t G) {
+  Plan p{};
+  if (count > 0 && rng > 0) {
+    const double q = ((double)rng + 1.0) / ((double)mask + 1.0);
+    p.Wi = (int64_t)ceil(count / q + 10.0 * sqrt(count * (1.0 - q)) / q) + 64;
+  }
+  if (G > 0) {
+    const double q = 0.78539816339744830962;
+    const double pairs = (double)((G + 1) / 2);
+    p.Aw = (int64_t)ceil(pairs / q + 10.0 * sqrt(pairs * (1.0 - q)) / q) + 64;
+  }
+  p.n_gen = (kN + p.Wi + 4 * p.Aw + kN - 1) / kN + 1;
+  p.nbI = (p.Wi + kIntPerBlock - 1) / kIntPerBlock;
+  p.nbA = (p.Aw + kAttPerBlock - 1) / kAttPerBlock;
+  Carver c(ws);
+  p.sc = c.take<Scalars>(1);
+  p.backup = c.take<uint32_t>(kN + 4);
+  p.raw = c.take<uint32_t>((size_t)(p.n_gen + 1) * kN);
+  p.cnt_i = c.take<int32_t>((size_t)p.nbI + 1);
+  p.cnt_a = c.take<int32_t>((size_t)p.nbA + 1);
+  p.bytes = c.bytes();
+  return p;
+}
+
+static int run_parallel(const Plan& p, uint32_t* state, int64_t count, int k, uint32_t rng, uint32_t mask,
+                        int32_t* idx, int64_t G, const Out& out, cudaStream_t stream) {
+  UMAPB_CUDA_TRY(cudaMemsetAsync(p.sc, 0, sizeof(Scalars), stream), "random draws: reset");
+  UMAPB_CUDA_TRY(cudaMemcpyAsync(p.backup, state, (kN + 4) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
+                 "random draws: state copy");
+  int launches = 3;
+  stream_kernel<<<1, kPar, 0, stream>>>(state, p.n_gen, p.raw);
+  if (count > 0 && rng == 0) {
+    const int64_t want = (count + 255) / 256;
+    const_ints_kernel<<<(unsigned)(want < 4096 ? want : 4096), 256, 0, stream>>>(count, k, idx);
+    ++launches;
+  } else if (count > 0) {
+    int_count_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i);
+    scan_exclusive_kernel<<<1, 1024, 0, stream>>>(p.cnt_i, p.nbI, &p.sc->tot_int);
+    int_scatter_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i, count, k, idx,
+                                                             p.sc);
+    launches += 3;
+  }
+  if (G > 0) {
+    att_count_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a);
+    scan_exclusive_kernel<<<1, 1024, 0, stream>>>(p.cnt_a, p.nbA, &p.sc->tot_att);
+    att_scatter_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a, G, out);
+    launches += 3;
+  }
+  final_state_kernel<<<1, kPar, 0, stream>>>(p.raw, state, p.sc, G);
+  // exits at once unless a margin fell short; then redoes every draw from the backup
+  walk_kernel<<<1, kThreads, 0, stream>>>(p.backup, state, &p.sc->status, k, count, rng, mask, idx, G, out);
+  UMAPB_LAUNCH_CHECK("random draws kernels");
+  count_launches(launches);
+  return UMAPB_OK;
+}
 }  // namespace rstart
 }  // namespace umapb
 
 using namespace umapb;
 
-extern "C" int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P,
-                                      int32_t pd1, float* P2, int32_t pd2, umapb_stream_t stream_) {
+static void mask_of(int64_t n, uint32_t* rng, uint32_t* mask) {
+  *rng = (uint32_t)(n - 2);  // randint(0, n - 1): values 0 .. n - 2
+  uint32_t m = *rng;
+  for (int s = 1; s <= 16; s <<= 1) m |= m >> s;
+  *mask = m;
+}
+
+extern "C" int umapb_nnd_random_start_workspace(int64_t n, int32_t k, int32_t d, int32_t pd1, int32_t pd2,
+                                                size_t* bytes) {
   clear_error();
+  UMAPB_REQUIRE(bytes && n >= 2 && n - 1 <= 0x7fffffff && k >= 1 && d >= 1 && pd1 >= 0 && pd2 >= 0,
+                "nnd_random_start_workspace: bad arguments");
+  uint32_t rng, mask;
+  mask_of(n, &rng, &mask);
+  *bytes = rstart::plan(nullptr, n * (int64_t)k, rng, mask, (int64_t)d * (pd1 + pd2)).bytes;
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P,
+                                      int32_t pd1, float* P2, int32_t pd2, void* workspace, size_t workspace_bytes,
+                                      umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(state && idx, "nnd_random_start: null state or idx");
   UMAPB_REQUIRE(n >= 2 && n - 1 <= 0x7fffffff && k >= 1 && d >= 1, "nnd_random_start: need n >= 2, k >= 1, d >= 1");
   UMAPB_REQUIRE(pd1 >= 0 && pd2 >= 0 && (pd1 == 0 || P) && (pd2 == 0 || P2),
                 "nnd_random_start: projection sizes must be >= 0 with their outputs given");
-  const uint32_t rng = (uint32_t)(n - 2);  // randint(0, n - 1): values 0 .. n - 2
-  uint32_t mask = rng;
-  for (int s = 1; s <= 16; s <<= 1) mask |= mask >> s;
+  uint32_t rng, mask;
+  mask_of(n, &rng, &mask);
   rstart::Out out;
   out.affine = 0;
   out.g1 = (int64_t)d * pd1;
@@ -254,16 +550,32 @@ extern "C" int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int
   out.P2 = P2;
   out.s2 = sqrt((double)(pd2 > 0 ? pd2 : 1));
   const int64_t G = out.g1 + (int64_t)d * pd2;
-  rstart::random_start_kernel<<<1, rstart::kThreads, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
-      state, k, n * (int64_t)k, rng, mask, idx, G, out);
+  const int64_t count = n * (int64_t)k;
+  if (workspace) {
+    const rstart::Plan need = rstart::plan(nullptr, count, rng, mask, G);
+    if (workspace_bytes < need.bytes)
+      return set_error(UMAPB_ERR_WORKSPACE, "nnd_random_start: workspace of %zu bytes, need %zu", workspace_bytes,
+                       need.bytes);
+    return rstart::run_parallel(rstart::plan(workspace, count, rng, mask, G), state, count, k, rng, mask, idx, G,
+                                out, stream);
+  }
+  rstart::walk_kernel<<<1, rstart::kThreads, 0, stream>>>(state, state, nullptr, k, count, rng, mask, idx, G, out);
   UMAPB_LAUNCH_CHECK("nnd_random_start kernel");
   count_launches(1);
   return UMAPB_OK;
 }
 
-extern "C" int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out,
-                                   umapb_stream_t stream_) {
+extern "C" int umapb_legacy_normal_workspace(int64_t count, size_t* bytes) {
   clear_error();
+  UMAPB_REQUIRE(bytes && count >= 0, "legacy_normal_workspace: bad arguments");
+  *bytes = rstart::plan(nullptr, 0, 1u, 1u, count).bytes;
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, double scale, float* out,
+                                   void* workspace, size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(state && (out || count == 0) && count >= 0, "legacy_normal: bad arguments");
   if (count == 0) return UMAPB_OK;
   rstart::Out o;
@@ -273,9 +585,16 @@ extern "C" int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, d
   o.s1 = loc;
   o.P2 = nullptr;
   o.s2 = scale;
-  // no bounded integers (count 0): the kernel goes straight to the normals
-  rstart::random_start_kernel<<<1, rstart::kThreads, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
-      state, 1, 0, 1u, 1u, nullptr, count, o);
+  if (workspace) {
+    const rstart::Plan need = rstart::plan(nullptr, 0, 1u, 1u, count);
+    if (workspace_bytes < need.bytes)
+      return set_error(UMAPB_ERR_WORKSPACE, "legacy_normal: workspace of %zu bytes, need %zu", workspace_bytes,
+                       need.bytes);
+    return rstart::run_parallel(rstart::plan(workspace, 0, 1u, 1u, count), state, 0, 1, 1u, 1u, nullptr, count, o,
+                                stream);
+  }
+  // no bounded integers (count 0): the walk goes straight to the normals
+  rstart::walk_kernel<<<1, rstart::kThreads, 0, stream>>>(state, state, nullptr, 1, 0, 1u, 1u, nullptr, count, o);
   UMAPB_LAUNCH_CHECK("legacy_normal kernel");
   count_launches(1);
   return UMAPB_OK;

@@ -133,12 +133,13 @@ def test_injected_negative_count_is_checked(golden, manifest):
         lay.epoch_injected(Y, 1, m["a"], m["b"], 1.0, 5, cuda(opt["neg_0"][:-5].astype(np.int32)))
 
 
-@pytest.mark.parametrize("seed,shape", [(42, (70000, 2)), (0, (1, 3)), (7, (2001, 2))])
-def test_device_legacy_normal_equals_numpy(seed, shape):
+@pytest.mark.parametrize("parallel", [True, False])
+@pytest.mark.parametrize("seed,shape", [(42, (70000, 2)), (0, (1, 3)), (7, (2001, 2)), (3, (1, 1))])
+def test_device_legacy_normal_equals_numpy(seed, shape, parallel):
     """The spectral init's noise, RandomState(seed).normal(scale=1e-4) as float32,
     drawn on the device from the stream's state, bit for bit."""
     from mlx_vis_b200 import _lib
 
     want = np.random.RandomState(seed).normal(scale=0.0001, size=shape).astype(np.float32)
-    got = _lib.legacy_normal(np.random.RandomState(seed), shape, 0.0, 0.0001, torch.device("cuda"))
+    got = _lib.legacy_normal(np.random.RandomState(seed), shape, 0.0, 0.0001, torch.device("cuda"), parallel=parallel)
     assert np.array_equal(got.cpu().numpy(), want)

@@ -101,16 +101,17 @@ def test_umap_with_nndescent(gauss2000):
     assert trustworthiness(gauss2000, Y, n_neighbors=15) > 0.95
 
 
+@pytest.mark.parametrize("parallel", [True, False])
 @pytest.mark.parametrize("n,k,d,seed", [(70000, 15, 784, 0), (5000, 15, 784, 3), (1000, 10, 150, 7), (257, 4, 64, 1),
                                         (2, 1, 5, 2), (3000, 32, 301, 11)])
-def test_device_random_start_equals_numpy(n, k, d, seed):
-    """umapb_nnd_random_start reproduces the reference's NumPy draws bit for bit
-    and leaves NumPy's global stream in the same state."""
+def test_device_random_start_equals_numpy(n, k, d, seed, parallel):
+    """umapb_nnd_random_start (grid-wide path and one-CTA walk) reproduces the
+    reference's NumPy draws bit for bit and leaves NumPy's stream in the same state."""
     from mlx_vis_b200._nndescent.nndescent import random_start, random_start_device, words_state
 
     idx_h, P_h, P2_h = random_start(n, k, d, seed)
     st_h = np.random.get_state()
-    idx, P, P2, state = random_start_device(n, k, d, seed, torch.device("cuda"))
+    idx, P, P2, state = random_start_device(n, k, d, seed, torch.device("cuda"), parallel=parallel)
     st = words_state(state.cpu().numpy())
     assert np.array_equal(idx.cpu().numpy(), idx_h)
     for got, want in ((P, P_h), (P2, P2_h)):
@@ -120,7 +121,8 @@ def test_device_random_start_equals_numpy(n, k, d, seed):
     assert np.array_equal(st[1], st_h[1]) and st[2:] == st_h[2:]
 
 
-def test_device_random_start_continues_an_unseeded_stream():
+@pytest.mark.parametrize("parallel", [True, False])
+def test_device_random_start_continues_an_unseeded_stream(parallel):
     """random_state=None: the draws continue NumPy's global stream, including a
     cached second normal (has_gauss) and a mid-generation position."""
     from mlx_vis_b200._nndescent.nndescent import random_start, random_start_device, words_state
@@ -133,7 +135,7 @@ def test_device_random_start_continues_an_unseeded_stream():
     idx_h, P_h, P2_h = random_start(900, 6, 350, None)
     st_h = np.random.get_state()
     np.random.set_state(st0)
-    idx, P, P2, state = random_start_device(900, 6, 350, None, torch.device("cuda"))
+    idx, P, P2, state = random_start_device(900, 6, 350, None, torch.device("cuda"), parallel=parallel)
     st = words_state(state.cpu().numpy())
     assert np.array_equal(idx.cpu().numpy(), idx_h)
     assert np.array_equal(P.cpu().numpy(), P_h) and np.array_equal(P2.cpu().numpy(), P2_h)
