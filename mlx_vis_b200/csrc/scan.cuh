@@ -6,18 +6,36 @@
 namespace umapb {
 
 // Exclusive scan of `count` int32 values in place by ONE block of 1024 threads;
-// writes the grand total to *total.
+// writes the grand total to *total.  Each pass covers 1024 x 8 values: a thread
+// scans its 8 consecutive values in registers (two 16-byte loads), the block scans
+// the thread sums (warp shuffles, then one warp over the 32 warp sums) and a
+// running carry links the passes.
 template <int kDummy = 0>
 __global__ void scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count, int64_t* __restrict__ total) {
+  constexpr int kItems = 8;
   __shared__ int64_t warp_sums[32];
   __shared__ int64_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t base = 0; base < count; base += blockDim.x) {
-    const int64_t idx = base + threadIdx.x;
-    const int64_t v = idx < count ? vals[idx] : 0;
-    int64_t x = v;
+  const int64_t span = (int64_t)blockDim.x * kItems;
+  const bool aligned = (reinterpret_cast<uintptr_t>(vals) & 15) == 0;
+  for (int64_t base = 0; base < count; base += span) {
+    const int64_t first = base + (int64_t)threadIdx.x * kItems;
+    int32_t v[kItems];
+    const bool full = aligned && first + kItems <= count;
+    if (full) {
+      const int4 a = *reinterpret_cast<const int4*>(vals + first);
+      const int4 b = *reinterpret_cast<const int4*>(vals + first + 4);
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    } else {
+#pragma unroll
+      for (int u = 0; u < kItems; ++u) v[u] = first + u < count ? vals[first + u] : 0;
+    }
+    int64_t sum = 0;
+#pragma unroll
+    for (int u = 0; u < kItems; ++u) sum += v[u];
+    int64_t x = sum;  // inclusive scan of the thread sums within the warp
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -35,10 +53,23 @@ __global__ void scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
       warp_sums[lane] = s;
     }
     __syncthreads();
-    const int64_t excl = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + x - v;
-    if (idx < count) vals[idx] = (int32_t)excl;
+    int64_t run = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
+    int32_t o[kItems];
+#pragma unroll
+    for (int u = 0; u < kItems; ++u) {
+      o[u] = (int32_t)run;
+      run += v[u];
+    }
+    if (full) {
+      *reinterpret_cast<int4*>(vals + first) = make_int4(o[0], o[1], o[2], o[3]);
+      *reinterpret_cast<int4*>(vals + first + 4) = make_int4(o[4], o[5], o[6], o[7]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < kItems; ++u)
+        if (first + u < count) vals[first + u] = o[u];
+    }
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    if (threadIdx.x == blockDim.x - 1) carry = run;
     __syncthreads();
   }
   if (threadIdx.x == 0) *total = carry;

@@ -7,11 +7,12 @@
 // min-max each column to [0, 10].
 //
 // Here the edges are in row-major order, so W V is a CSR SpMV without atomics
-// (one thread per row, edges summed in the reference's order).  MGS of the
+// (8 lanes per row, FP64 partial sums combined by shuffles).  MGS of the
 // (c+1)-column block equals Q = V R^-1 with R the Cholesky factor of the Gram
 // matrix V^T V (+1e-10 on each pivot, as in the reference's norms), so each
 // iteration is ONE kernel: it applies the previous iteration's R^-1 to every
-// gathered row on the fly and accumulates the new Gram matrix in FP64.
+// gathered row on the fly and accumulates the new Gram matrix in FP64; its last
+// block factors that Gram matrix for the next iteration.
 #include <math.h>
 
 #include "common.cuh"
@@ -22,6 +23,7 @@ namespace spectral {
 
 constexpr int kBlock = 256;
 constexpr int kMaxCols = 5;  // n_components <= 4
+constexpr int kLanes = 8;    // lanes per row in the power iteration
 
 __global__ void row_ptr_kernel(const int32_t* __restrict__ rows, const int64_t* __restrict__ n_edges, int64_t n,
                                int64_t* __restrict__ row_ptr) {
@@ -81,26 +83,29 @@ __device__ void chol_inverse(const double* G, int kk, double* ri) {
   }
 }
 
-// One power iteration: Vout = W (Vin Rinv_prev); G_out += Vout^T Vout.
-// G_prev == nullptr means Rinv = I (the first multiplication uses V0 as is).
-__global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* __restrict__ G_prev,
+// One power iteration: Vout = W (Vin Rinv_in); G_out += Vout^T Vout.  Rinv_in ==
+// nullptr means the identity (the first multiplication uses V0 as is).  kLanes
+// lanes per row stride over its edges (rows of the symmetrised graph range from a
+// few edges to hundreds) and meet by shuffles.  The last block to finish (a counter
+// per iteration) factors the completed G_out once and writes Rinv_out for the next
+// iteration.
+__global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* __restrict__ Rinv_in,
                                  const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
                                  const float* __restrict__ wn, int64_t n, int kk, double* __restrict__ Vout,
-                                 double* __restrict__ G_out) {
+                                 double* __restrict__ G_out, unsigned* __restrict__ counter,
+                                 double* __restrict__ Rinv_out) {
   __shared__ double ri[kMaxCols * kMaxCols];
   __shared__ double gsum[kBlock / 32][kMaxCols * kMaxCols];
-  if (threadIdx.x == 0) {
-    if (G_prev) {
-      chol_inverse(G_prev, kk, ri);
-    } else {
-      for (int i = 0; i < kk * kk; ++i) ri[i] = (i % (kk + 1) == 0) ? 1.0 : 0.0;
-    }
-  }
+  __shared__ bool last;
+  if (threadIdx.x < kk * kk)
+    ri[threadIdx.x] = Rinv_in ? Rinv_in[threadIdx.x] : ((threadIdx.x % (kk + 1) == 0) ? 1.0 : 0.0);
   __syncthreads();
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int sub = threadIdx.x & (kLanes - 1);
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kLanes;
   double acc[kMaxCols] = {0, 0, 0, 0, 0};
   if (r < n) {
-    for (int64_t e = row_ptr[r]; e < row_ptr[r + 1]; ++e) {
+    const int64_t e1 = row_ptr[r + 1];
+    for (int64_t e = row_ptr[r] + sub; e < e1; e += kLanes) {
       const int64_t c = cols[e];
       const double w = (double)wn[e];
       double v[kMaxCols];
@@ -111,8 +116,15 @@ __global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* _
         acc[j] += w * q;
       }
     }
-    for (int j = 0; j < kk; ++j) Vout[r * kk + j] = acc[j];
   }
+  for (int j = 0; j < kk; ++j) {
+#pragma unroll
+    for (int o = kLanes / 2; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+  }
+  if (r < n && sub == 0)
+    for (int j = 0; j < kk; ++j) Vout[r * kk + j] = acc[j];
+  if (sub != 0)
+    for (int j = 0; j < kk; ++j) acc[j] = 0.0;  // one copy of each row in the Gram sum
   // block reduction of the Gram matrix
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int i = 0; i < kk; ++i) {
@@ -133,6 +145,16 @@ __global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* _
       if (i != j) atomicAdd(&G_out[j * kk + i], g);
     }
   }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double G[kMaxCols * kMaxCols];
+    for (int i = 0; i < kk * kk; ++i) G[i] = __ldcg(G_out + i);
+    chol_inverse(G, kk, Rinv_out);
+  }
 }
 
 __device__ __forceinline__ unsigned f2ord(float f) {
@@ -144,10 +166,10 @@ __device__ __forceinline__ float ord2f(unsigned u) {
 }
 
 // embedding = (V R^-1)[:, 1:], max |embedding|
-__global__ void finish_orth_kernel(const double* __restrict__ V, const double* __restrict__ G, int64_t n, int kk,
+__global__ void finish_orth_kernel(const double* __restrict__ V, const double* __restrict__ Rinv, int64_t n, int kk,
                                    float* __restrict__ emb, unsigned* __restrict__ absmax) {
   __shared__ double ri[kMaxCols * kMaxCols];
-  if (threadIdx.x == 0) chol_inverse(G, kk, ri);
+  if (threadIdx.x < kk * kk) ri[threadIdx.x] = Rinv[threadIdx.x];
   __syncthreads();
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   float m = 0.f;
@@ -198,7 +220,9 @@ struct Layout {
   float* dis;
   float* wn;
   double* V[2];
-  double* G;  // n_iter blocks of kk*kk
+  double* G;       // n_iter blocks of kk*kk
+  double* Rinv;    // n_iter blocks of kk*kk: the inverse Cholesky factor after each iteration
+  unsigned* done;  // per-iteration block counters
   float* emb;
   unsigned* red;  // absmax, colmin[4], colmax[4]
   size_t bytes;
@@ -215,6 +239,8 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   l.V[0] = c.take<double>((size_t)n * kk);
   l.V[1] = c.take<double>((size_t)n * kk);
   l.G = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
+  l.Rinv = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
+  l.done = c.take<unsigned>((size_t)(n_iter > 0 ? n_iter : 1));
   l.emb = c.take<float>((size_t)n * dim);
   l.red = c.take<unsigned>(16);
   l.bytes = c.bytes();
@@ -283,6 +309,7 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   const unsigned rb = (unsigned)ceil_div(n, spectral::kBlock);
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.status, 0, 4, stream), "spectral: status reset");
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.G, 0, sizeof(double) * n_iter * kk * kk, stream), "spectral: gram reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.done, 0, sizeof(unsigned) * n_iter, stream), "spectral: counter reset");
   spectral::row_ptr_kernel<<<(unsigned)ceil_div(n + 1, spectral::kBlock), spectral::kBlock, 0, stream>>>(
       rows, n_edges, n, l.row_ptr);
   spectral::degree_kernel<<<rb, spectral::kBlock, 0, stream>>>(vals, l.row_ptr, n, l.dis);
@@ -292,17 +319,18 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   spectral::f32_to_f64_kernel<<<(unsigned)ceil_div(n * kk, spectral::kBlock), spectral::kBlock, 0, stream>>>(
       V0, l.V[0], n * kk);
   UMAPB_LAUNCH_CHECK("spectral: setup kernels");
+  const unsigned pb = (unsigned)ceil_div(n * spectral::kLanes, spectral::kBlock);
   for (int it = 0; it < n_iter; ++it) {
-    const double* gprev = it == 0 ? nullptr : l.G + (size_t)(it - 1) * kk * kk;
-    spectral::spmv_gram_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[it & 1], gprev, l.row_ptr, cols, l.wn, n,
-                                                                     kk, l.V[(it + 1) & 1],
-                                                                     l.G + (size_t)it * kk * kk);
+    const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
+    spectral::spmv_gram_kernel<<<pb, spectral::kBlock, 0, stream>>>(
+        l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk, l.done + it,
+        l.Rinv + (size_t)it * kk * kk);
   }
   UMAPB_LAUNCH_CHECK("spectral: power iteration");
   spectral::init_red_kernel<<<1, 32, 0, stream>>>(l.red, dim);
   spectral::finish_orth_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[n_iter & 1],
-                                                                     l.G + (size_t)(n_iter - 1) * kk * kk, n, kk,
-                                                                     l.emb, l.red);
+                                                                     l.Rinv + (size_t)(n_iter - 1) * kk * kk, n,
+                                                                     kk, l.emb, l.red);
   const unsigned eb = (unsigned)ceil_div(n * dim, spectral::kBlock);
   spectral::scale_noise_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, noise, n, dim, l.red, l.red + 1,
                                                                      l.red + 5);
