@@ -224,7 +224,8 @@ class UMAP:
 
 
 class _Events:
-    """Per-stage CUDA-event timings (milliseconds) collected without extra syncs."""
+    """Per-stage CUDA-event timings (milliseconds) collected without extra syncs,
+    with the host time at which each stage finished issuing its work (host_ keys)."""
 
     def __init__(self, dev):
         self.dev = dev
@@ -232,11 +233,13 @@ class _Events:
         self.start = torch.cuda.Event(enable_timing=True)
         self.start.record()
         self.marks = []
+        self.host = []
 
     def mark(self, name):
         e = torch.cuda.Event(enable_timing=True)
         e.record()
         self.marks.append((name, e))
+        self.host.append((name, time.perf_counter()))
 
     def finish(self):
         torch.cuda.synchronize(self.dev)
@@ -247,4 +250,8 @@ class _Events:
             prev = e
         out["total_device"] = self.start.elapsed_time(prev)
         out["total_wall"] = (time.perf_counter() - self.t0) * 1000.0
+        t = self.t0
+        for name, h in self.host:
+            out["host_" + name] = (h - t) * 1000.0
+            t = h
         return out

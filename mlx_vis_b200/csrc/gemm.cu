@@ -4,21 +4,28 @@
 //
 //   C[M, N] = sum_k A[m, k] B[n, k]      A (M x K), B (N x K): BF16, K-major
 //
-// One CTA per 128 x 128 output tile: warp 0 streams 64-wide K blocks of A and B
-// with TMA (128-byte swizzle, zero fill past M, N, K) through 4 stages, one thread
-// of warp 1 issues tcgen05.mma (M=128, N=128, K=16, FP32 accumulation in TMEM),
-// warps 2-5 (one per TMEM lane quarter) read the accumulator with tcgen05.ld and
-// apply the epilogue:
-//   EPI_F32        C (f32, row-major, pitch ldc)
+// One CTA per 128 x 128 output tile and K slice (gridDim.z slices of the K
+// blocks; the F32 epilogue then adds its partial tile to C with atomics): warp 0
+// streams 64-wide K blocks of A and B with TMA (128-byte swizzle, zero fill past
+// M, N, K) through 4 stages, one thread of warp 1 issues tcgen05.mma (M=128, N=128,
+// K=16, FP32 accumulation in TMEM), warps 2-5 (one per TMEM lane quarter) read the
+// accumulator with tcgen05.ld, 32 columns at a time, and apply the epilogue:
+//   EPI_F32        C (f32, row-major, pitch ldc), stored or (K slices) accumulated
 //   EPI_BIAS_GELU  z = C + bias[n]; Z (f32), H = bf16(gelu(z)) row-major and,
 //                  when HT != null, its transpose H^T (N x M, pitch ldt)
-//   EPI_GELU_BACK  g = C; dZ = g * gelu'(Z) -> bf16 row-major and transpose
-// gelu(z) = z * Phi(z) (exact, erf); gelu'(z) = Phi(z) + z phi(z).
+//   EPI_GELU_BACK  g = C; dZ = g * gelu'(Z) -> bf16 row-major, optional transpose,
+//                  optional column sums of the bf16 values in colsum
+// The accumulator rows sit one per thread; each 32 x 32 chunk passes through
+// shared memory (the drained operand stages) so row-major outputs are written a
+// row per warp instruction, and the transposed output straight from the row
+// layout, a column per instruction.
+// gelu(z) = z * Phi(z); gelu'(z) = Phi(z) + z phi(z) (gelu.cuh).
 // Every mbarrier wait is bounded (2 s) and reports through *status.
 #include <cuda_bf16.h>
 #include <math.h>
 
 #include "common.cuh"
+#include "gelu.cuh"
 #include "tc.cuh"
 
 namespace umapb {
@@ -42,14 +49,10 @@ struct EpiArgs {
   int ldh;
   __nv_bfloat16* HT;      // optional bf16 transposed output (N x M, pitch ldt)
   int ldt;
+  float* colsum;          // EPI_GELU_BACK: optional column sums of H (atomic adds)
+  int accumulate;         // EPI_F32: add to C with atomics (K split over gridDim.z)
 };
 
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
-__device__ __forceinline__ float gelu_grad(float z) {
-  const float cdf = 0.5f * (1.0f + erff(z * 0.70710678118654752f));
-  const float pdf = 0.39894228040143268f * expf(-0.5f * z * z);
-  return cdf + z * pdf;
-}
 
 template <int EPI>
 __global__ void __launch_bounds__(THREADS, 1)
@@ -65,6 +68,10 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // this CTA's K blocks [kb0, kb1); the host sizes the slices so none is empty
+  const int per = (num_kb + gridDim.z - 1) / gridDim.z;
+  const int kb0 = blockIdx.z * per;
+  const int kb1 = kb0 + per < num_kb ? kb0 + per : num_kb;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -87,9 +94,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      for (int kb = 0; kb < num_kb; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      for (int kb = kb0; kb < kb1; ++kb) {
+        const int i = kb - kb0;
+        const int s = i % STAGES;
+        const uint32_t ph = (uint32_t)(i / STAGES) & 1u;
         if (!tc::mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
         uint8_t* sa = smem + s * STAGE_BYTES;
         tc::mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
@@ -101,9 +109,10 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (lane == 0) {
       constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
       bool ok = true;
-      for (int kb = 0; kb < num_kb; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+      for (int kb = kb0; kb < kb1; ++kb) {
+        const int i = kb - kb0;
+        const int s = i % STAGES;
+        const uint32_t ph = (uint32_t)(i / STAGES) & 1u;
         if (!tc::mbar_wait(&full[s], ph, abort_flag)) {
           ok = false;
           break;
@@ -114,16 +123,18 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
         for (int k = 0; k < BK / UK; ++k)
           tc::mma_bf16(tmem_base, tc::sw128_kmajor_desc(a_addr + k * 32), tc::sw128_kmajor_desc(b_addr + k * 32),
-                       idesc, (kb | k) != 0 ? 1u : 0u);
+                       idesc, (i | k) != 0 ? 1u : 0u);
         tc::mma_commit(&empty[s]);
       }
       if (ok) tc::mma_commit(done);
     }
   } else {
-    // epilogue: thread = accumulator row (TMEM lane), 32 columns per tcgen05.ld
+    // epilogue: thread = accumulator row (TMEM lane), 32 columns per tcgen05.ld,
+    // staged through this warp's 32 x 33 float tile in the drained stage memory
+    // (every MMA, and so every TMA load, has completed once `done` fires)
     const int q = warp & 3;
-    const int r = q * 32 + lane;
-    const int m = m0 + r;
+    const int rbase = m0 + q * 32;  // first row of this warp's quarter
+    float* S = reinterpret_cast<float*>(smem) + q * 32 * 33;
     if (tc::mbar_wait(done, 0, abort_flag)) {
       tc::tc_fence_after();
       for (int ch = 0; ch < BN / 32; ++ch) {
@@ -131,25 +142,42 @@ __global__ void __launch_bounds__(THREADS, 1)
         __syncwarp();
         tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ch * 32), v);
         const int nb = n0 + ch * 32;
-        if (m < e.M) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int n = nb + j;
-            if (n >= e.N) break;
-            if (EPI == EPI_F32) {
-              e.C[(int64_t)m * e.ldc + n] = v[j];
-            } else if (EPI == EPI_BIAS_GELU) {
-              const float z = v[j] + e.bias[n];
-              e.Z[(int64_t)m * e.ldz + n] = z;
-              const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
-              e.H[(int64_t)m * e.ldh + n] = h;
-              if (e.HT) e.HT[(int64_t)n * e.ldt + m] = h;
-            } else {
-              const float dz = v[j] * gelu_grad(e.Z[(int64_t)m * e.ldz + n]);
-              const __nv_bfloat16 h = __float2bfloat16_rn(dz);
-              e.H[(int64_t)m * e.ldh + n] = h;
-              if (e.HT) e.HT[(int64_t)n * e.ldt + m] = h;
-            }
+        for (int j = 0; j < 32; ++j) S[lane * 33 + j] = v[j];
+        __syncwarp();
+        // column phase: lane = column n, one accumulator row per step
+        const int n = nb + lane;
+        const bool nin = n < e.N;
+        float bias_n = 0.f, csum = 0.f;
+        if (EPI == EPI_BIAS_GELU && nin) bias_n = e.bias[n];
+        for (int rr = 0; rr < 32; ++rr) {
+          const int m = rbase + rr;
+          if (m >= e.M || !nin) continue;
+          const float val = S[rr * 33 + lane];
+          if (EPI == EPI_F32) {
+            if (e.accumulate) atomicAdd(&e.C[(int64_t)m * e.ldc + n], val);
+            else e.C[(int64_t)m * e.ldc + n] = val;
+          } else if (EPI == EPI_BIAS_GELU) {
+            const float z = val + bias_n;
+            e.Z[(int64_t)m * e.ldz + n] = z;
+            const __nv_bfloat16 h = __float2bfloat16_rn(gelu(z));
+            e.H[(int64_t)m * e.ldh + n] = h;
+            S[rr * 33 + lane] = __bfloat162float(h);
+          } else {
+            const __nv_bfloat16 h = __float2bfloat16_rn(val * gelu_grad(e.Z[(int64_t)m * e.ldz + n]));
+            e.H[(int64_t)m * e.ldh + n] = h;
+            const float hf = __bfloat162float(h);
+            S[rr * 33 + lane] = hf;
+            csum += hf;
+          }
+        }
+        if (EPI == EPI_GELU_BACK && e.colsum && nin) atomicAdd(&e.colsum[n], csum);
+        if (EPI != EPI_F32 && e.HT) {  // row phase: lane = row m, one column per step
+          __syncwarp();
+          const int m = rbase + lane;
+          if (m < e.M) {
+            for (int j = 0; j < 32 && nb + j < e.N; ++j)
+              e.HT[(int64_t)(nb + j) * e.ldt + m] = __float2bfloat16_rn(S[lane * 33 + j]);
           }
         }
       }
@@ -165,7 +193,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 template <int EPI>
-static int launch(const void* A, const void* B, int M, int N, int K, int lda, int ldb, const EpiArgs& e,
+static int launch(const void* A, const void* B, int M, int N, int K, int lda, int ldb, int ksplit, const EpiArgs& e,
                   int32_t* status, cudaStream_t stream) {
   static bool attr[64] = {false};
   int dev = 0;
@@ -179,8 +207,11 @@ static int launch(const void* A, const void* B, int M, int N, int K, int lda, in
   int s;
   if ((s = make_tmap_bf16_2d(&ta, A, (uint64_t)M, (uint64_t)K, (uint64_t)lda, BM, BK))) return s;
   if ((s = make_tmap_bf16_2d(&tb, B, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, BN, BK))) return s;
-  dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN));
-  gemm_kernel<EPI><<<grid, THREADS, SMEM, stream>>>(ta, tb, (int)ceil_div(K, BK), e, status);
+  const int num_kb = (int)ceil_div(K, BK);
+  const int per = (int)ceil_div(num_kb, ksplit);
+  const int slices = (int)ceil_div(num_kb, per);  // every slice gets at least one K block
+  dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN), (unsigned)slices);
+  gemm_kernel<EPI><<<grid, THREADS, SMEM, stream>>>(ta, tb, num_kb, e, status);
   UMAPB_LAUNCH_CHECK("gemm kernel launch");
   count_launches(1);
   return UMAPB_OK;
@@ -192,29 +223,34 @@ static int launch(const void* A, const void* B, int M, int N, int K, int lda, in
 using namespace umapb;
 
 extern "C" int umapb_gemm_bf16(const void* A, const void* B, int32_t M, int32_t N, int32_t K, int32_t lda,
-                               int32_t ldb, int32_t epilogue, float* C, int32_t ldc, const float* bias, float* Z,
-                               int32_t ldz, void* H, int32_t ldh, void* HT, int32_t ldt, int32_t* status,
-                               umapb_stream_t stream_) {
+                               int32_t ldb, int32_t epilogue, int32_t ksplit, float* C, int32_t ldc, const float* bias,
+                               float* Z, int32_t ldz, void* H, int32_t ldh, void* HT, int32_t ldt, float* colsum,
+                               int32_t* status, umapb_stream_t stream_) {
   clear_error();
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(A && B && status, "gemm: null operand");
   UMAPB_REQUIRE(M >= 1 && N >= 1 && K >= 1, "gemm: empty shape");
   UMAPB_REQUIRE(lda >= K && ldb >= K && lda % 8 == 0 && ldb % 8 == 0,
                 "gemm: lda/ldb must be >= K and multiples of 8 elements (16-byte rows)");
+  UMAPB_REQUIRE(ksplit >= 1 && ksplit <= 64, "gemm: ksplit must be in [1, 64]");
+  UMAPB_REQUIRE(ksplit == 1 || epilogue == gemm::EPI_F32, "gemm: K slices need the F32 epilogue");
   gemm::EpiArgs e{M, N, C, ldc, bias, Z, ldz, static_cast<__nv_bfloat16*>(H), ldh, static_cast<__nv_bfloat16*>(HT),
-                  ldt};
+                  ldt, colsum, ksplit > 1 ? 1 : 0};
   switch (epilogue) {
     case gemm::EPI_F32:
       UMAPB_REQUIRE(C && ldc >= N, "gemm: EPI_F32 needs C with ldc >= N");
-      return gemm::launch<gemm::EPI_F32>(A, B, M, N, K, lda, ldb, e, status, stream);
+      if (ksplit > 1)
+        UMAPB_CUDA_TRY(cudaMemsetAsync(C, 0, sizeof(float) * ((size_t)(M - 1) * ldc + N), stream), "gemm: C reset");
+      return gemm::launch<gemm::EPI_F32>(A, B, M, N, K, lda, ldb, ksplit, e, status, stream);
     case gemm::EPI_BIAS_GELU:
       UMAPB_REQUIRE(bias && Z && H && ldz >= N && ldh >= N && (!HT || ldt >= M),
                     "gemm: EPI_BIAS_GELU needs bias, Z and H (and ldt >= M for HT)");
-      return gemm::launch<gemm::EPI_BIAS_GELU>(A, B, M, N, K, lda, ldb, e, status, stream);
+      return gemm::launch<gemm::EPI_BIAS_GELU>(A, B, M, N, K, lda, ldb, 1, e, status, stream);
     case gemm::EPI_GELU_BACK:
       UMAPB_REQUIRE(Z && H && ldz >= N && ldh >= N && (!HT || ldt >= M),
                     "gemm: EPI_GELU_BACK needs Z and H (and ldt >= M for HT)");
-      return gemm::launch<gemm::EPI_GELU_BACK>(A, B, M, N, K, lda, ldb, e, status, stream);
+      if (colsum) UMAPB_CUDA_TRY(cudaMemsetAsync(colsum, 0, sizeof(float) * N, stream), "gemm: colsum reset");
+      return gemm::launch<gemm::EPI_GELU_BACK>(A, B, M, N, K, lda, ldb, 1, e, status, stream);
     default:
       return set_error(UMAPB_ERR_ARG, "gemm: unknown epilogue %d", epilogue);
   }

@@ -8,10 +8,12 @@ it provides the starting layout, so optimize_layout needs fewer epochs, and
 ``enc.transform(X_new)`` embeds unseen rows without a fit.
 
 Numerics: FP32 master weights and Adam moments; the two hidden layers run as
-tcgen05 BF16 GEMMs with FP32 accumulation and fused bias + exact GELU
-(libumap_b200 ``umapb_gemm_bf16``); the c-wide output layer keeps FP32 weights.
-The training loss is the mean squared error per row.  Every step is a sequence
-of library kernels (forward, backward, AdamW) — no autograd.
+tcgen05 BF16 GEMMs with FP32 accumulation and fused bias + GELU (erf-based GELU,
+erf to 1.5e-7 by Abramowitz & Stegun 7.1.26; libumap_b200 ``umapb_gemm_bf16``);
+the c-wide output layer keeps FP32 weights.  The training loss is the mean
+squared error per row.  Every step is a sequence of library kernels (forward,
+backward with split-K weight gradients, one AdamW launch) — no autograd — and
+``fit`` replays it as one CUDA graph per batch.
 """
 
 from __future__ import annotations
@@ -63,6 +65,7 @@ class Encoder:
         self.W2bT = torch.empty((h, h), dtype=bf, device=self.dev)
         self._refresh_bf16()
         self.status = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.step_t = torch.zeros(1, dtype=torch.int32, device=self.dev)  # AdamW step number on the device
         self._buf = {}
         self.history_ = []
         self.y_scale_ = None  # (mean, std) of the targets the encoder was trained on
@@ -86,7 +89,6 @@ class Encoder:
         if train:
             b.update({"XT": torch.zeros((self.d, ldb), dtype=bf, device=dev),
                       "H1T": torch.zeros((h, ldb), dtype=bf, device=dev),
-                      "H2T": torch.zeros((h, ldb), dtype=bf, device=dev),
                       "dY": torch.empty((B, c), device=dev), "dZ2": torch.empty((B, h), dtype=bf, device=dev),
                       "dZ2T": torch.zeros((h, ldb), dtype=bf, device=dev),
                       "dZ1": torch.empty((B, h), dtype=bf, device=dev),
@@ -96,9 +98,9 @@ class Encoder:
         return b
 
     def _gemm(self, A, Bm, M, N, K, lda, ldb, epi, C=None, ldc=0, bias=None, Z=None, ldz=0, H=None, ldh=0, HT=None,
-              ldt=0):
-        call("umapb_gemm_bf16", ptr(A), ptr(Bm), M, N, K, lda, ldb, epi, ptr(C), ldc, ptr(bias), ptr(Z), ldz, ptr(H),
-             ldh, ptr(HT), ldt, ptr(self.status), stream_handle())
+              ldt=0, ksplit=1, colsum=None):
+        call("umapb_gemm_bf16", ptr(A), ptr(Bm), M, N, K, lda, ldb, epi, ksplit, ptr(C), ldc, ptr(bias), ptr(Z), ldz,
+             ptr(H), ldh, ptr(HT), ldt, ptr(colsum), ptr(self.status), stream_handle())
 
     def _forward(self, X: torch.Tensor, b, train: bool):
         B = X.shape[0]
@@ -107,8 +109,7 @@ class Encoder:
              b["ldb"], s)
         self._gemm(b["Xb"], self.W1b, B, h, self.d, self.ldx, self.ldx, BIAS_GELU, bias=p["b1"], Z=b["Z1"], ldz=h,
                    H=b["H1"], ldh=h, HT=b["H1T"] if train else None, ldt=b["ldb"])
-        self._gemm(b["H1"], self.W2b, B, h, h, h, h, BIAS_GELU, bias=p["b2"], Z=b["Z2"], ldz=h, H=b["H2"], ldh=h,
-                   HT=b["H2T"] if train else None, ldt=b["ldb"])
+        self._gemm(b["H1"], self.W2b, B, h, h, h, h, BIAS_GELU, bias=p["b2"], Z=b["Z2"], ldz=h, H=b["H2"], ldh=h)
         call("umapb_mlp_head_forward", ptr(b["H2"]), h, B, h, ptr(p["W3"]), ptr(p["b3"]), self.c, ptr(b["Y"]), s)
         return b["Y"]
 
@@ -122,43 +123,58 @@ class Encoder:
         b = self._buffers(B, True)
         s = stream_handle()
         self._forward(X, b, True)
-        call("umapb_mlp_head_backward", ptr(b["Y"]), ptr(T), B, c, ptr(p["W3"]), h, ptr(b["Z2"]), h, ptr(b["H2T"]),
-             b["ldb"], ptr(b["dY"]), ptr(g["W3"]), ptr(g["b3"]), ptr(b["dZ2"]), h, ptr(b["dZ2T"]), ptr(b["loss"]), s)
-        # dW2 = dZ2^T H1, db2
-        self._gemm(b["dZ2T"], b["H1T"], h, h, B, b["ldb"], b["ldb"], F32, C=g["W2"], ldc=h)
-        call("umapb_mlp_rowsum", ptr(b["dZ2T"]), h, B, b["ldb"], ptr(g["b2"]), s)
-        # dZ1 = (dZ2 W2) * gelu'(Z1)
+        # dY, loss, dW3, db3, dZ2 (+ transpose), db2
+        call("umapb_mlp_head_backward", ptr(b["Y"]), ptr(T), B, c, ptr(p["W3"]), h, ptr(b["Z2"]), h, ptr(b["H2"]), h,
+             ptr(b["dY"]), ptr(g["W3"]), ptr(g["b3"]), ptr(b["dZ2"]), h, ptr(b["dZ2T"]), b["ldb"], ptr(g["b2"]),
+             ptr(b["loss"]), s)
+        # dW2 = dZ2^T H1 (K = B split over CTAs)
+        self._gemm(b["dZ2T"], b["H1T"], h, h, B, b["ldb"], b["ldb"], F32, C=g["W2"], ldc=h, ksplit=self._ksplit(B))
+        # dZ1 = (dZ2 W2) * gelu'(Z1) (+ transpose), db1 = its column sums
         self._gemm(b["dZ2"], self.W2bT, B, h, h, h, h, GELU_BACK, Z=b["Z1"], ldz=h, H=b["dZ1"], ldh=h, HT=b["dZ1T"],
-                   ldt=b["ldb"])
-        # dW1 = dZ1^T X, db1
-        self._gemm(b["dZ1T"], b["XT"], h, d, B, b["ldb"], b["ldb"], F32, C=g["W1"], ldc=d)
-        call("umapb_mlp_rowsum", ptr(b["dZ1T"]), h, B, b["ldb"], ptr(g["b1"]), s)
+                   ldt=b["ldb"], colsum=g["b1"])
+        # dW1 = dZ1^T X
+        self._gemm(b["dZ1T"], b["XT"], h, d, B, b["ldb"], b["ldb"], F32, C=g["W1"], ldc=d, ksplit=self._ksplit(B))
         self.step_count += 1
+        self.step_t.add_(1)
         self._adamw()
         return b["loss"]
 
+    @staticmethod
+    def _ksplit(K: int) -> int:
+        """K slices for the weight-gradient GEMMs (K = batch): about 8 K blocks of 64 each."""
+        return max(1, min(16, (K + 511) // 512))
+
     def _adamw(self):
+        """One launch for all parameter groups (umapb_adamw)."""
+        if getattr(self, "_adamw_args", None) is None:
+            import ctypes
+
+            names = list(self.params)
+            n = len(names)
+            P = ctypes.c_void_p * n
+            I = ctypes.c_int32 * n
+            bf = {"W1": (self.W1b, self.ldx, None, 0), "W2": (self.W2b, self.h, self.W2bT, self.h)}
+            shp = [(t.shape[0], t.shape[1]) if t.dim() == 2 else (1, t.shape[0]) for t in self.params.values()]
+            self._adamw_args = (
+                n, P(*[ptr(self.params[k]) for k in names]), P(*[ptr(self.grads[k]) for k in names]),
+                P(*[ptr(self.m[k]) for k in names]), P(*[ptr(self.v[k]) for k in names]),
+                I(*[r for r, _ in shp]), I(*[c for _, c in shp]),
+                P(*[ptr(bf[k][0]) if k in bf else None for k in names]), I(*[bf[k][1] if k in bf else 0 for k in names]),
+                P(*[ptr(bf[k][2]) if k in bf else None for k in names]), I(*[bf[k][3] if k in bf else 0 for k in names]))
         b1, b2 = self.betas
-        s = stream_handle()
-        for name, prm in self.params.items():
-            rows, cols = (prm.shape[0], prm.shape[1]) if prm.dim() == 2 else (1, prm.shape[0])
-            pb, ldb, pbt, ldbt = None, 0, None, 0
-            if name == "W1":
-                pb, ldb = self.W1b, self.ldx
-            elif name == "W2":
-                pb, ldb, pbt, ldbt = self.W2b, self.h, self.W2bT, self.h
-            call("umapb_adamw", ptr(prm), ptr(self.grads[name]), ptr(self.m[name]), ptr(self.v[name]), rows, cols,
-                 float(self.lr), float(b1), float(b2), float(self.eps), float(self.wd), self.step_count, ptr(pb), ldb,
-                 ptr(pbt), ldbt, s)
+        call("umapb_adamw", *self._adamw_args, float(self.lr), float(b1), float(b2), float(self.eps), float(self.wd),
+             ptr(self.step_t), stream_handle())
 
     def check_status(self):
         if int(self.status.item()) != 0:
             raise _lib.UmapB200Error("umapb_gemm_bf16", 5, "device-side wait expired in a GEMM")
 
     # ------------------------------------------------------------------
-    def fit(self, Xs, Ys, epochs: int = 20, verbose: bool = False, seed: int = 0):
+    def fit(self, Xs, Ys, epochs: int = 20, verbose: bool = False, seed: int = 0, use_graph: bool = True):
         """Trains on the (X, Y) pairs (lists of arrays or tensors); targets are standardised
-        with their global mean / std, which transform() undoes."""
+        with their global mean / std, which transform() undoes.  With ``use_graph`` the
+        training step (batch gather, forward, backward, AdamW) is recorded once into a
+        CUDA graph and replayed for every batch after the first."""
         Xd = torch.cat([to_device_f32(x, self.dev) for x in Xs])
         Yd = torch.cat([to_device_f32(y, self.dev) for y in Ys])
         mean = Yd.mean(dim=0)
@@ -169,13 +185,36 @@ class Encoder:
         gen = torch.Generator(device=self.dev)
         gen.manual_seed(seed)
         B = min(self.batch_size, n)
+        nb = n // B
+        sel = torch.empty(B, dtype=torch.int64, device=self.dev)  # the batch's row indices
+        total = torch.zeros((), device=self.dev)
+
+        def step():
+            loss = self.train_step(torch.index_select(Xd, 0, sel), torch.index_select(Yn, 0, sel))
+            total.add_(loss[0])
+
+        graph = None
         for ep in range(epochs):
             perm = torch.randperm(n, device=self.dev, generator=gen)
-            total = torch.zeros((), device=self.dev)
-            nb = n // B
+            total.zero_()
             for i in range(nb):
-                sel = perm[i * B:(i + 1) * B]
-                total += self.train_step(Xd[sel], Yn[sel])[0]
+                sel.copy_(perm[i * B:(i + 1) * B])
+                if graph is not None:
+                    graph.replay()
+                    self.step_count += 1
+                    continue
+                step()  # eager: the first batch (it also sets up every buffer the capture reuses)
+                if use_graph and nb * epochs > 1:
+                    graph = torch.cuda.CUDAGraph()
+                    side = torch.cuda.Stream()
+                    side.wait_stream(torch.cuda.current_stream())
+                    with torch.cuda.stream(side):
+                        count = self.step_count
+                        graph.capture_begin()
+                        step()
+                        graph.capture_end()
+                        self.step_count = count  # capturing records the step without running it
+                    torch.cuda.current_stream().wait_stream(side)
             self.history_.append(float(total.item()) / max(nb, 1))
             if verbose:
                 print(f"encoder epoch {ep + 1}/{epochs}: loss {self.history_[-1]:.4f}")

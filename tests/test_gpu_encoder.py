@@ -10,29 +10,33 @@ from oracle import mlp as omlp
 pytestmark = pytest.mark.gpu
 
 
-def gemm(A, B, epi=0, bias=None, Z=None, with_t=False):
+def gemm(A, B, epi=0, bias=None, Z=None, with_t=False, ksplit=1, colsum=False):
     from mlx_vis_b200 import _lib
 
     M, K = A.shape
     N = B.shape[0]
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
-    C = torch.empty((M, N), device="cuda") if epi == 0 else None
+    C = torch.full((M, N), float("nan"), device="cuda") if epi == 0 else None
     H = torch.empty((M, N), dtype=torch.bfloat16, device="cuda") if epi else None
     HT = torch.empty((N, M), dtype=torch.bfloat16, device="cuda") if (epi and with_t) else None
     Zo = torch.empty((M, N), device="cuda") if epi == 1 else Z
-    _lib.call("umapb_gemm_bf16", _lib.ptr(A), _lib.ptr(B), M, N, K, A.stride(0), B.stride(0), epi, _lib.ptr(C), N,
-              _lib.ptr(bias), _lib.ptr(Zo), N, _lib.ptr(H), N, _lib.ptr(HT), M, _lib.ptr(st), _lib.stream_handle())
+    cs = torch.full((N,), float("nan"), device="cuda") if colsum else None
+    _lib.call("umapb_gemm_bf16", _lib.ptr(A), _lib.ptr(B), M, N, K, A.stride(0), B.stride(0), epi, ksplit,
+              _lib.ptr(C), N, _lib.ptr(bias), _lib.ptr(Zo), N, _lib.ptr(H), N, _lib.ptr(HT), M, _lib.ptr(cs),
+              _lib.ptr(st), _lib.stream_handle())
     torch.cuda.synchronize()
     assert int(st.item()) == 0
-    return C, Zo, H, HT
+    return (C, Zo, H, HT, cs) if colsum else (C, Zo, H, HT)
 
 
-@pytest.mark.parametrize("M,N,K", [(300, 200, 104), (4096, 512, 784), (512, 784, 4096), (128, 128, 64), (1, 8, 8)])
-def test_gemm_f32_matches_float64(M, N, K):
+@pytest.mark.parametrize("ksplit", [1, 8])
+@pytest.mark.parametrize("M,N,K", [(300, 200, 104), (4096, 512, 784), (512, 784, 4096), (128, 128, 64), (1, 8, 8),
+                                   (512, 512, 4000)])
+def test_gemm_f32_matches_float64(M, N, K, ksplit):
     g = torch.Generator().manual_seed(M + N + K)
     A = torch.randn((M, K), generator=g).to(torch.bfloat16)
     B = torch.randn((N, K), generator=g).to(torch.bfloat16)
-    C, *_ = gemm(A.cuda(), B.cuda())
+    C, *_ = gemm(A.cuda(), B.cuda(), ksplit=ksplit)
     ref = A.double() @ B.double().T
     err = (C.cpu().double() - ref).abs().max() / ref.abs().max()
     assert err < 1e-5
@@ -50,13 +54,15 @@ def test_gemm_epilogues_match_float64():
     assert (Z.cpu().double() - z).abs().max() < 1e-4
     assert (H.cpu().double() - h).abs().max() < 1e-2 * max(1.0, float(h.abs().max()))
     assert torch.equal(HT.cpu(), H.cpu().T)
-    # backward epilogue: dZ = C * gelu'(Z)
-    _, _, dZ, dZT = gemm(A.cuda(), B.cuda(), epi=2, Z=Z, with_t=True)
+    # backward epilogue: dZ = C * gelu'(Z), with the column sums of the bf16 values
+    _, _, dZ, dZT, cs = gemm(A.cuda(), B.cuda(), epi=2, Z=Z, with_t=True, colsum=True)
     zz = z.clone().requires_grad_(True)
     torch.nn.functional.gelu(zz).backward(torch.ones_like(zz))
     ref = (A.double() @ B.double().T) * zz.grad
     assert (dZ.cpu().double() - ref).abs().max() < 1e-2 * max(1.0, float(ref.abs().max()))
     assert torch.equal(dZT.cpu(), dZ.cpu().T)
+    want = dZ.cpu().double().sum(0)
+    assert (cs.cpu().double() - want).abs().max() < 1e-4 * max(1.0, float(want.abs().max()))
 
 
 def _params(enc):
