@@ -230,15 +230,18 @@ int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, const int32_t*
  * umapb_gemm_bf16: C[M,N] = sum_k A[m,k] B[n,k] on tcgen05 tensor cores, A and B
  *   BF16 row-major with pitches lda, ldb (multiples of 8, >= K), FP32 accumulation,
  *   fused epilogue: UMAPB_GEMM_F32 (C, ldc; with ksplit > 1 the K blocks are split
- *   over ksplit CTAs per tile and C, zeroed by the call, accumulates them with
- *   atomics); UMAPB_GEMM_BIAS_GELU (Z = C + bias, H = bf16(gelu(Z)), optional H^T);
+ *   over ksplit CTAs per tile and C holds ksplit slices of M x ldc, slice s at
+ *   C + s M ldc, whose sum is the product); UMAPB_GEMM_BIAS_GELU (Z = C + bias,
+ *   H = bf16(gelu(Z)), optional H^T);
  *   UMAPB_GEMM_GELU_BACK (H = bf16(C * gelu'(Z)), optional H^T, optional column
  *   sums of H in colsum, zeroed by the call).  *status (device int32) reports an
  *   expired bounded wait.
- * umapb_mlp_convert: X f32 (rows x d) -> BF16 (rows x ldx, zero padded) and an
+ * umapb_mlp_convert: X f32 (rows x d; row r taken from row row_idx[r] when row_idx,
+ *   a device int64 array, is given) -> BF16 (rows x ldx, zero padded) and an
  *   optional transposed BF16 copy (d x rows, pitch ldt).
  * umapb_mlp_head_forward: Y = H W^T + b for the last layer (c <= 4, FP32 W).
- * umapb_mlp_head_backward: MSE loss mean_b |Y - T|^2 (device f32), dY, dW = dY^T H2,
+ * umapb_mlp_head_backward: MSE loss mean_b |Y - T|^2 (device f32; T row t_idx[b] when
+ *   the device int64 array t_idx is given), dY, dW = dY^T H2,
  *   db = sum dY, dZ2 = bf16((dY W) * gelu'(Z2)) row-major and transposed, and
  *   dbias2 = column sums of dZ2 (loss, dW, db, dbias2 zeroed by the call).
  * umapb_adamw: decoupled-weight-decay Adam on n_groups (<= 8) FP32 master
@@ -246,6 +249,9 @@ int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, const int32_t*
  *   corrected at the step number *step (device memory, so a captured step can
  *   replay), writing optional BF16 copies (p_bf16 / ldb) and transposed BF16
  *   copies (p_bf16_t / ldbt); p_bf16 / p_bf16_t may be null or hold null entries.
+ *   With g_slices (host array, may be null) group k's gradient is the sum of
+ *   g_slices[k] slices g[k] + s g_stride[k] (the K-sliced GEMM output); the sum
+ *   is written back to the first slice.
  * ------------------------------------------------------------------------- */
 #define UMAPB_GEMM_F32 0
 #define UMAPB_GEMM_BIAS_GELU 1
@@ -254,16 +260,18 @@ int umapb_gemm_bf16(const void* A, const void* B, int32_t M, int32_t N, int32_t 
                     int32_t epilogue, int32_t ksplit, float* C, int32_t ldc, const float* bias, float* Z, int32_t ldz,
                     void* H, int32_t ldh, void* HT, int32_t ldt, float* colsum, int32_t* status,
                     umapb_stream_t stream);
-int umapb_mlp_convert(const float* X, int32_t rows, int32_t d, int32_t ldx, void* Xb, void* XT, int32_t ldt,
-                      umapb_stream_t stream);
+int umapb_mlp_convert(const float* X, const int64_t* row_idx, int32_t rows, int32_t d, int32_t ldx, void* Xb,
+                      void* XT, int32_t ldt, umapb_stream_t stream);
 int umapb_mlp_head_forward(const void* H, int32_t ldh, int32_t B, int32_t Hd, const float* W, const float* bias,
                            int32_t c, float* Y, umapb_stream_t stream);
-int umapb_mlp_head_backward(const float* Y, const float* T, int32_t B, int32_t c, const float* W, int32_t Hd,
+int umapb_mlp_head_backward(const float* Y, const float* T, const int64_t* t_idx, int32_t B, int32_t c,
+                            const float* W, int32_t Hd,
                             const float* Z2, int32_t ldz, const void* H2, int32_t ldh2, float* dY, float* dW,
                             float* db, void* dZ2, int32_t lddz, void* dZ2T, int32_t ldt, float* dbias2, float* loss,
                             umapb_stream_t stream);
-int umapb_adamw(int32_t n_groups, float* const* p, const float* const* g, float* const* m, float* const* v,
-                const int32_t* rows, const int32_t* cols, void* const* p_bf16, const int32_t* ldb,
+int umapb_adamw(int32_t n_groups, float* const* p, float* const* g, const int32_t* g_slices,
+                const int64_t* g_stride, float* const* m, float* const* v, const int32_t* rows, const int32_t* cols,
+                void* const* p_bf16, const int32_t* ldb,
                 void* const* p_bf16_t, const int32_t* ldbt, float lr, float beta1, float beta2, float eps,
                 float weight_decay, const int32_t* step, umapb_stream_t stream);
 

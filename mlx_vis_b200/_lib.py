@@ -49,11 +49,11 @@ SIGNATURES = {
     "umapb_kernel_launches": [],
     "umapb_gemm_bf16": [_p, _p, _i32, _i32, _i32, _i32, _i32, _i32, _i32, _p, _i32, _p, _p, _i32, _p, _i32, _p,
                         _i32, _p, _p, _p],
-    "umapb_mlp_convert": [_p, _i32, _i32, _i32, _p, _p, _i32, _p],
+    "umapb_mlp_convert": [_p, _p, _i32, _i32, _i32, _p, _p, _i32, _p],
     "umapb_mlp_head_forward": [_p, _i32, _i32, _i32, _p, _p, _i32, _p, _p],
-    "umapb_mlp_head_backward": [_p, _p, _i32, _i32, _p, _i32, _p, _i32, _p, _i32, _p, _p, _p, _p, _i32, _p, _i32,
-                                _p, _p, _p],
-    "umapb_adamw": [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _f32, _f32, _f32, _f32, _f32, _p, _p],
+    "umapb_mlp_head_backward": [_p, _p, _p, _i32, _i32, _p, _i32, _p, _i32, _p, _i32, _p, _p, _p, _p, _i32, _p,
+                                _i32, _p, _p, _p],
+    "umapb_adamw": [_i32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _f32, _f32, _f32, _f32, _f32, _p, _p],
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
     "umapb_nnd_random_start_workspace": [_i64, _i32, _i32, _i32, _i32, _psz],
     "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p, _sz, _p],

@@ -5,12 +5,13 @@
 //   C[M, N] = sum_k A[m, k] B[n, k]      A (M x K), B (N x K): BF16, K-major
 //
 // One CTA per 128 x 128 output tile and K slice (gridDim.z slices of the K
-// blocks; the F32 epilogue then adds its partial tile to C with atomics): warp 0
+// blocks; the F32 epilogue then writes each slice's partial tile to its own
+// M x ldc block of C, for the consumer to sum): warp 0
 // streams 64-wide K blocks of A and B with TMA (128-byte swizzle, zero fill past
 // M, N, K) through 4 stages, one thread of warp 1 issues tcgen05.mma (M=128, N=128,
 // K=16, FP32 accumulation in TMEM), warps 2-5 (one per TMEM lane quarter) read the
 // accumulator with tcgen05.ld, 32 columns at a time, and apply the epilogue:
-//   EPI_F32        C (f32, row-major, pitch ldc), stored or (K slices) accumulated
+//   EPI_F32        C (f32, row-major, pitch ldc); with K slices, slice z at C + z M ldc
 //   EPI_BIAS_GELU  z = C + bias[n]; Z (f32), H = bf16(gelu(z)) row-major and,
 //                  when HT != null, its transpose H^T (N x M, pitch ldt)
 //   EPI_GELU_BACK  g = C; dZ = g * gelu'(Z) -> bf16 row-major, optional transpose,
@@ -50,7 +51,7 @@ struct EpiArgs {
   __nv_bfloat16* HT;      // optional bf16 transposed output (N x M, pitch ldt)
   int ldt;
   float* colsum;          // EPI_GELU_BACK: optional column sums of H (atomic adds)
-  int accumulate;         // EPI_F32: add to C with atomics (K split over gridDim.z)
+  int64_t slice;          // EPI_F32 with K slices: slice z is written at C + z * slice
 };
 
 
@@ -150,13 +151,18 @@ __global__ void __launch_bounds__(THREADS, 1)
         const bool nin = n < e.N;
         float bias_n = 0.f, csum = 0.f;
         if (EPI == EPI_BIAS_GELU && nin) bias_n = e.bias[n];
+        float zpre[32];  // GELU_BACK: this column's 32 pre-activations, all loads issued first
+        if (EPI == EPI_GELU_BACK) {
+#pragma unroll
+          for (int rr = 0; rr < 32; ++rr)
+            zpre[rr] = (nin && rbase + rr < e.M) ? e.Z[(int64_t)(rbase + rr) * e.ldz + n] : 0.f;
+        }
         for (int rr = 0; rr < 32; ++rr) {
           const int m = rbase + rr;
           if (m >= e.M || !nin) continue;
           const float val = S[rr * 33 + lane];
           if (EPI == EPI_F32) {
-            if (e.accumulate) atomicAdd(&e.C[(int64_t)m * e.ldc + n], val);
-            else e.C[(int64_t)m * e.ldc + n] = val;
+            e.C[blockIdx.z * e.slice + (int64_t)m * e.ldc + n] = val;
           } else if (EPI == EPI_BIAS_GELU) {
             const float z = val + bias_n;
             e.Z[(int64_t)m * e.ldz + n] = z;
@@ -164,7 +170,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             e.H[(int64_t)m * e.ldh + n] = h;
             S[rr * 33 + lane] = __bfloat162float(h);
           } else {
-            const __nv_bfloat16 h = __float2bfloat16_rn(val * gelu_grad(e.Z[(int64_t)m * e.ldz + n]));
+            const __nv_bfloat16 h = __float2bfloat16_rn(val * gelu_grad(zpre[rr]));
             e.H[(int64_t)m * e.ldh + n] = h;
             const float hf = __bfloat162float(h);
             S[rr * 33 + lane] = hf;
@@ -210,6 +216,10 @@ static int launch(const void* A, const void* B, int M, int N, int K, int lda, in
   const int num_kb = (int)ceil_div(K, BK);
   const int per = (int)ceil_div(num_kb, ksplit);
   const int slices = (int)ceil_div(num_kb, per);  // every slice gets at least one K block
+  if (slices < ksplit)  // the caller sums ksplit slices: the ones without K blocks hold zeros
+    UMAPB_CUDA_TRY(cudaMemsetAsync(e.C + slices * e.slice, 0, sizeof(float) * (size_t)(ksplit - slices) * e.slice,
+                                   stream),
+                   "gemm: empty slices");
   dim3 grid((unsigned)ceil_div(M, BM), (unsigned)ceil_div(N, BN), (unsigned)slices);
   gemm_kernel<EPI><<<grid, THREADS, SMEM, stream>>>(ta, tb, num_kb, e, status);
   UMAPB_LAUNCH_CHECK("gemm kernel launch");
@@ -235,12 +245,10 @@ extern "C" int umapb_gemm_bf16(const void* A, const void* B, int32_t M, int32_t 
   UMAPB_REQUIRE(ksplit >= 1 && ksplit <= 64, "gemm: ksplit must be in [1, 64]");
   UMAPB_REQUIRE(ksplit == 1 || epilogue == gemm::EPI_F32, "gemm: K slices need the F32 epilogue");
   gemm::EpiArgs e{M, N, C, ldc, bias, Z, ldz, static_cast<__nv_bfloat16*>(H), ldh, static_cast<__nv_bfloat16*>(HT),
-                  ldt, colsum, ksplit > 1 ? 1 : 0};
+                  ldt, colsum, (int64_t)M * ldc};
   switch (epilogue) {
     case gemm::EPI_F32:
       UMAPB_REQUIRE(C && ldc >= N, "gemm: EPI_F32 needs C with ldc >= N");
-      if (ksplit > 1)
-        UMAPB_CUDA_TRY(cudaMemsetAsync(C, 0, sizeof(float) * ((size_t)(M - 1) * ldc + N), stream), "gemm: C reset");
       return gemm::launch<gemm::EPI_F32>(A, B, M, N, K, lda, ldb, ksplit, e, status, stream);
     case gemm::EPI_BIAS_GELU:
       UMAPB_REQUIRE(bias && Z && H && ldz >= N && ldh >= N && (!HT || ldt >= M),

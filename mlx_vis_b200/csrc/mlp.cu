@@ -28,15 +28,16 @@ namespace mlp {
 constexpr int kMaxOut = 4;
 
 // X (rows x d, f32) -> Xb (rows x ldx bf16, zero padded) and optional XT (d x rows bf16, pitch ldt)
-__global__ void convert_kernel(const float* __restrict__ X, int rows, int d, int ldx, __nv_bfloat16* __restrict__ Xb,
-                               __nv_bfloat16* __restrict__ XT, int ldt) {
+// (row r of the outputs reads row row_idx[r] of X when row_idx is given)
+__global__ void convert_kernel(const float* __restrict__ X, const int64_t* __restrict__ row_idx, int rows, int d,
+                               int ldx, __nv_bfloat16* __restrict__ Xb, __nv_bfloat16* __restrict__ XT, int ldt) {
   __shared__ float tile[32][33];
   const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int i = ty; i < 32; i += 8) {
     const int r = r0 + i, c = c0 + tx;
     float v = 0.f;
-    if (r < rows && c < d) v = X[(int64_t)r * d + c];
+    if (r < rows && c < d) v = X[(row_idx ? row_idx[r] : (int64_t)r) * d + c];
     if (r < rows && c < ldx) Xb[(int64_t)r * ldx + c] = __float2bfloat16_rn(v);
     tile[i][tx] = v;
   }
@@ -87,13 +88,15 @@ __global__ void head_forward_kernel(const __nv_bfloat16* __restrict__ H, int ldh
 
 // One block per 32 rows x 128 columns (8 warps, 4 rows each; a lane owns 4 adjacent
 // columns):
-//   g = dY[b] = 2 (Y[b] - T[b]) / B and the loss (column block 0 only),
+//   g = dY[b] = 2 (Y[b] - T[b]) / B (T row t_idx[b] when given) and the loss
+//   (column block 0 only),
 //   dZ2 = bf16((g W) * gelu'(Z2)) row-major, and transposed through shared memory,
 //   dW += g^T H2, db += sum g (column block 0), dbias2 += column sums of dZ2,
 // the sums accumulated with atomics (the host entry zeroes them first).
 constexpr int kHbRows = 32, kHbCols = 128;
 __global__ void __launch_bounds__(256) head_backward_kernel(
-    const float* __restrict__ Y, const float* __restrict__ T, int B, int c, const float* __restrict__ W, int Hd,
+    const float* __restrict__ Y, const float* __restrict__ T, const int64_t* __restrict__ t_idx, int B, int c,
+    const float* __restrict__ W, int Hd,
     const float* __restrict__ Z, int ldz, const __nv_bfloat16* __restrict__ H2, int ldh2, float* __restrict__ dY,
     float* __restrict__ dW, float* __restrict__ db, __nv_bfloat16* __restrict__ dZ, int lddz,
     __nv_bfloat16* __restrict__ dZT, int ldt, float* __restrict__ dbias2, float* __restrict__ loss) {
@@ -108,7 +111,7 @@ __global__ void __launch_bounds__(256) head_backward_kernel(
     for (int o = 0; o < kMaxOut; ++o) {
       float gv = 0.f;
       if (b < B && o < c) {
-        const float diff = Y[(int64_t)b * c + o] - T[(int64_t)b * c + o];
+        const float diff = Y[(int64_t)b * c + o] - T[(t_idx ? t_idx[b] : (int64_t)b) * c + o];
         gv = 2.0f * diff / (float)B;
         l += diff * diff;
         if (blockIdx.x == 0) dY[(int64_t)b * c + o] = gv;
@@ -214,7 +217,8 @@ __global__ void __launch_bounds__(256) head_backward_kernel(
 }
 
 // Decoupled-weight-decay Adam (AdamW) on FP32 masters, every parameter group in one
-// launch; optional BF16 copy (rows x cols, pitch ldb) and transposed BF16 copy
+// launch; a group's gradient may arrive as K slices (summed here, the sum kept in
+// slice 0); optional BF16 copy (rows x cols, pitch ldb) and transposed BF16 copy
 // (cols x rows, pitch ldbt).  The step number t comes from device memory, so a
 // captured training step replays with the current count; bias corrections 1 - beta^t.
 constexpr int kMaxGroups = 8;
@@ -222,7 +226,9 @@ struct AdamwGroups {
   int n;
   int64_t start[kMaxGroups + 1];  // offsets of the groups in the flattened index space
   float* p[kMaxGroups];
-  const float* g[kMaxGroups];
+  float* g[kMaxGroups];
+  int nsplit[kMaxGroups];          // gradient = sum of nsplit slices, stride apart
+  int64_t stride[kMaxGroups];
   float* m[kMaxGroups];
   float* v[kMaxGroups];
   int cols[kMaxGroups];
@@ -241,7 +247,11 @@ __global__ void adamw_kernel(AdamwGroups G, float lr, float beta1, float beta2, 
     int k = 0;
     while (k + 1 < G.n && t >= G.start[k + 1]) ++k;
     const int i = (int)(t - G.start[k]);  // a group holds < 2^31 values
-    const float gr = G.g[k][i];
+    float gr = G.g[k][i];
+    if (G.nsplit[k] > 1) {  // K-sliced gradient: sum the slices, keep the sum in slice 0
+      for (int sl = 1; sl < G.nsplit[k]; ++sl) gr += G.g[k][i + sl * G.stride[k]];
+      G.g[k][i] = gr;
+    }
     const float mt = beta1 * G.m[k][i] + (1.0f - beta1) * gr;
     const float vt = beta2 * G.v[k][i] + (1.0f - beta2) * gr * gr;
     G.m[k][i] = mt;
@@ -267,14 +277,14 @@ static unsigned grid_for(int64_t work, int per_block) {
   return (unsigned)(b < cap ? b : cap);
 }
 
-extern "C" int umapb_mlp_convert(const float* X, int32_t rows, int32_t d, int32_t ldx, void* Xb, void* XT,
-                                 int32_t ldt, umapb_stream_t stream) {
+extern "C" int umapb_mlp_convert(const float* X, const int64_t* row_idx, int32_t rows, int32_t d, int32_t ldx,
+                                 void* Xb, void* XT, int32_t ldt, umapb_stream_t stream) {
   clear_error();
   UMAPB_REQUIRE(X && Xb && rows >= 1 && d >= 1 && ldx >= d, "mlp_convert: bad arguments");
   UMAPB_REQUIRE(!XT || ldt >= rows, "mlp_convert: ldt must be >= rows");
   dim3 grid((unsigned)ceil_div(ldx, 32), (unsigned)ceil_div(rows, 32)), block(32, 8);
   mlp::convert_kernel<<<grid, block, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      X, rows, d, ldx, static_cast<__nv_bfloat16*>(Xb), static_cast<__nv_bfloat16*>(XT), ldt);
+      X, row_idx, rows, d, ldx, static_cast<__nv_bfloat16*>(Xb), static_cast<__nv_bfloat16*>(XT), ldt);
   UMAPB_LAUNCH_CHECK("mlp_convert kernel");
   count_launches(1);
   return UMAPB_OK;
@@ -295,7 +305,8 @@ extern "C" int umapb_mlp_head_forward(const void* H, int32_t ldh, int32_t B, int
   return UMAPB_OK;
 }
 
-extern "C" int umapb_mlp_head_backward(const float* Y, const float* T, int32_t B, int32_t c, const float* W,
+extern "C" int umapb_mlp_head_backward(const float* Y, const float* T, const int64_t* t_idx, int32_t B, int32_t c,
+                                       const float* W,
                                        int32_t Hd, const float* Z2, int32_t ldz, const void* H2, int32_t ldh2,
                                        float* dY, float* dW, float* db, void* dZ2, int32_t lddz, void* dZ2T,
                                        int32_t ldt, float* dbias2, float* loss, umapb_stream_t stream_) {
@@ -311,7 +322,7 @@ extern "C" int umapb_mlp_head_backward(const float* Y, const float* T, int32_t B
   UMAPB_CUDA_TRY(cudaMemsetAsync(db, 0, sizeof(float) * c, stream), "mlp_head_backward: db reset");
   UMAPB_CUDA_TRY(cudaMemsetAsync(dbias2, 0, sizeof(float) * Hd, stream), "mlp_head_backward: dbias2 reset");
   dim3 grid((unsigned)ceil_div(Hd, mlp::kHbCols), (unsigned)ceil_div(B, mlp::kHbRows));
-  mlp::head_backward_kernel<<<grid, 256, 0, stream>>>(Y, T, B, c, W, Hd, Z2, ldz,
+  mlp::head_backward_kernel<<<grid, 256, 0, stream>>>(Y, T, t_idx, B, c, W, Hd, Z2, ldz,
                                                       static_cast<const __nv_bfloat16*>(H2), ldh2, dY, dW, db,
                                                       static_cast<__nv_bfloat16*>(dZ2), lddz,
                                                       static_cast<__nv_bfloat16*>(dZ2T), ldt, dbias2, loss);
@@ -320,8 +331,9 @@ extern "C" int umapb_mlp_head_backward(const float* Y, const float* T, int32_t B
   return UMAPB_OK;
 }
 
-extern "C" int umapb_adamw(int32_t n_groups, float* const* p, const float* const* g, float* const* m,
-                           float* const* v, const int32_t* rows, const int32_t* cols, void* const* p_bf16,
+extern "C" int umapb_adamw(int32_t n_groups, float* const* p, float* const* g, const int32_t* g_slices,
+                           const int64_t* g_stride, float* const* m, float* const* v, const int32_t* rows,
+                           const int32_t* cols, void* const* p_bf16,
                            const int32_t* ldb, void* const* p_bf16_t, const int32_t* ldbt, float lr, float beta1,
                            float beta2, float eps, float weight_decay, const int32_t* step, umapb_stream_t stream) {
   clear_error();
@@ -339,6 +351,10 @@ extern "C" int umapb_adamw(int32_t n_groups, float* const* p, const float* const
     UMAPB_REQUIRE(!pbt || ldbt[k] >= rows[k], "adamw: ldbt must be >= rows");
     G.p[k] = p[k];
     G.g[k] = g[k];
+    G.nsplit[k] = g_slices ? g_slices[k] : 1;
+    G.stride[k] = g_slices ? g_stride[k] : 0;
+    UMAPB_REQUIRE(G.nsplit[k] >= 1 && (G.nsplit[k] == 1 || G.stride[k] >= (int64_t)rows[k] * cols[k]),
+                  "adamw: gradient slices need a stride >= rows * cols");
     G.m[k] = m[k];
     G.v[k] = v[k];
     G.cols[k] = cols[k];

@@ -35,6 +35,8 @@ def _pad8(x: int) -> int:
 class Encoder:
     """MLP encoder trained on (X, Y) pairs of UMAP embeddings."""
 
+    KSPLIT_MAX = 16
+
     def __init__(self, in_dim: int, hidden: int = 512, out_dim: int = 2, lr: float = 1e-3,
                  weight_decay: float = 1e-2, betas=(0.9, 0.999), eps: float = 1e-8, batch_size: int = 4096,
                  seed: int = 0):
@@ -59,6 +61,12 @@ class Encoder:
         self.m = {k: torch.zeros_like(v) for k, v in self.params.items()}
         self.v = {k: torch.zeros_like(v) for k, v in self.params.items()}
         self.grads = {k: torch.empty_like(v) for k, v in self.params.items()}
+        # W1 and W2 gradients arrive as K slices of the split-K GEMMs (AdamW sums them
+        # into slice 0, which is grads[...] afterwards)
+        self._gpart = {"W1": torch.empty((self.KSPLIT_MAX, h, d), device=self.dev),
+                       "W2": torch.empty((self.KSPLIT_MAX, h, h), device=self.dev)}
+        for k, t in self._gpart.items():
+            self.grads[k] = t[0]
         bf = torch.bfloat16
         self.W1b = torch.zeros((h, self.ldx), dtype=bf, device=self.dev)
         self.W2b = torch.empty((h, h), dtype=bf, device=self.dev)
@@ -102,11 +110,11 @@ class Encoder:
         call("umapb_gemm_bf16", ptr(A), ptr(Bm), M, N, K, lda, ldb, epi, ksplit, ptr(C), ldc, ptr(bias), ptr(Z), ldz,
              ptr(H), ldh, ptr(HT), ldt, ptr(colsum), ptr(self.status), stream_handle())
 
-    def _forward(self, X: torch.Tensor, b, train: bool):
-        B = X.shape[0]
+    def _forward(self, X: torch.Tensor, b, train: bool, rows=None):
+        B = X.shape[0] if rows is None else rows.numel()
         h, p, s = self.h, self.params, stream_handle()
-        call("umapb_mlp_convert", ptr(X), B, self.d, self.ldx, ptr(b["Xb"]), ptr(b["XT"] if train else None),
-             b["ldb"], s)
+        call("umapb_mlp_convert", ptr(X), ptr(rows), B, self.d, self.ldx, ptr(b["Xb"]),
+             ptr(b["XT"] if train else None), b["ldb"], s)
         self._gemm(b["Xb"], self.W1b, B, h, self.d, self.ldx, self.ldx, BIAS_GELU, bias=p["b1"], Z=b["Z1"], ldz=h,
                    H=b["H1"], ldh=h, HT=b["H1T"] if train else None, ldt=b["ldb"])
         self._gemm(b["H1"], self.W2b, B, h, h, h, h, BIAS_GELU, bias=p["b2"], Z=b["Z2"], ldz=h, H=b["H2"], ldh=h)
@@ -114,38 +122,41 @@ class Encoder:
         return b["Y"]
 
     # ------------------------------------------------------------------
-    def train_step(self, X: torch.Tensor, T: torch.Tensor) -> torch.Tensor:
-        """One AdamW step on a batch (device float32 X (B, d), T (B, c)); returns the loss (device)."""
+    def train_step(self, X: torch.Tensor, T: torch.Tensor, rows=None) -> torch.Tensor:
+        """One AdamW step on a batch; returns the loss (device).  X (B, d) and T (B, c)
+        are device float32; with ``rows`` (device int64) they are whole sets and the
+        batch is their rows ``rows``, gathered by the kernels."""
         X = X.contiguous()
         T = T.contiguous()
-        B = X.shape[0]
+        B = X.shape[0] if rows is None else rows.numel()
         h, d, c, p, g = self.h, self.d, self.c, self.params, self.grads
         b = self._buffers(B, True)
         s = stream_handle()
-        self._forward(X, b, True)
+        ks = self._ksplit(B)
+        self._forward(X, b, True, rows)
         # dY, loss, dW3, db3, dZ2 (+ transpose), db2
-        call("umapb_mlp_head_backward", ptr(b["Y"]), ptr(T), B, c, ptr(p["W3"]), h, ptr(b["Z2"]), h, ptr(b["H2"]), h,
-             ptr(b["dY"]), ptr(g["W3"]), ptr(g["b3"]), ptr(b["dZ2"]), h, ptr(b["dZ2T"]), b["ldb"], ptr(g["b2"]),
-             ptr(b["loss"]), s)
-        # dW2 = dZ2^T H1 (K = B split over CTAs)
-        self._gemm(b["dZ2T"], b["H1T"], h, h, B, b["ldb"], b["ldb"], F32, C=g["W2"], ldc=h, ksplit=self._ksplit(B))
+        call("umapb_mlp_head_backward", ptr(b["Y"]), ptr(T), ptr(rows), B, c, ptr(p["W3"]), h, ptr(b["Z2"]), h,
+             ptr(b["H2"]), h, ptr(b["dY"]), ptr(g["W3"]), ptr(g["b3"]), ptr(b["dZ2"]), h, ptr(b["dZ2T"]), b["ldb"],
+             ptr(g["b2"]), ptr(b["loss"]), s)
+        # dW2 = dZ2^T H1 (K = B in ks slices)
+        self._gemm(b["dZ2T"], b["H1T"], h, h, B, b["ldb"], b["ldb"], F32, C=self._gpart["W2"], ldc=h, ksplit=ks)
         # dZ1 = (dZ2 W2) * gelu'(Z1) (+ transpose), db1 = its column sums
         self._gemm(b["dZ2"], self.W2bT, B, h, h, h, h, GELU_BACK, Z=b["Z1"], ldz=h, H=b["dZ1"], ldh=h, HT=b["dZ1T"],
                    ldt=b["ldb"], colsum=g["b1"])
-        # dW1 = dZ1^T X
-        self._gemm(b["dZ1T"], b["XT"], h, d, B, b["ldb"], b["ldb"], F32, C=g["W1"], ldc=d, ksplit=self._ksplit(B))
+        # dW1 = dZ1^T X (K = B in ks slices)
+        self._gemm(b["dZ1T"], b["XT"], h, d, B, b["ldb"], b["ldb"], F32, C=self._gpart["W1"], ldc=d, ksplit=ks)
         self.step_count += 1
         self.step_t.add_(1)
-        self._adamw()
+        self._adamw(ks)
         return b["loss"]
 
-    @staticmethod
-    def _ksplit(K: int) -> int:
+    @classmethod
+    def _ksplit(cls, K: int) -> int:
         """K slices for the weight-gradient GEMMs (K = batch): about 8 K blocks of 64 each."""
-        return max(1, min(16, (K + 511) // 512))
+        return max(1, min(cls.KSPLIT_MAX, (K + 511) // 512))
 
-    def _adamw(self):
-        """One launch for all parameter groups (umapb_adamw)."""
+    def _adamw(self, ks: int):
+        """One launch for all parameter groups (umapb_adamw); W1 and W2 gradients in ks slices."""
         if getattr(self, "_adamw_args", None) is None:
             import ctypes
 
@@ -155,15 +166,23 @@ class Encoder:
             I = ctypes.c_int32 * n
             bf = {"W1": (self.W1b, self.ldx, None, 0), "W2": (self.W2b, self.h, self.W2bT, self.h)}
             shp = [(t.shape[0], t.shape[1]) if t.dim() == 2 else (1, t.shape[0]) for t in self.params.values()]
+            self._adamw_names = names
+            self._adamw_stride = (ctypes.c_int64 * n)(*[self.params[k].numel() if k in self._gpart else 0
+                                                        for k in names])
             self._adamw_args = (
                 n, P(*[ptr(self.params[k]) for k in names]), P(*[ptr(self.grads[k]) for k in names]),
                 P(*[ptr(self.m[k]) for k in names]), P(*[ptr(self.v[k]) for k in names]),
                 I(*[r for r, _ in shp]), I(*[c for _, c in shp]),
                 P(*[ptr(bf[k][0]) if k in bf else None for k in names]), I(*[bf[k][1] if k in bf else 0 for k in names]),
                 P(*[ptr(bf[k][2]) if k in bf else None for k in names]), I(*[bf[k][3] if k in bf else 0 for k in names]))
+        import ctypes
+
+        slices = (ctypes.c_int32 * len(self._adamw_names))(*[ks if k in self._gpart else 1
+                                                             for k in self._adamw_names])
+        n, pp, gg, mm, vv, *rest = self._adamw_args
         b1, b2 = self.betas
-        call("umapb_adamw", *self._adamw_args, float(self.lr), float(b1), float(b2), float(self.eps), float(self.wd),
-             ptr(self.step_t), stream_handle())
+        call("umapb_adamw", n, pp, gg, slices, self._adamw_stride, mm, vv, *rest, float(self.lr), float(b1), float(b2),
+             float(self.eps), float(self.wd), ptr(self.step_t), stream_handle())
 
     def check_status(self):
         if int(self.status.item()) != 0:
@@ -173,7 +192,7 @@ class Encoder:
     def fit(self, Xs, Ys, epochs: int = 20, verbose: bool = False, seed: int = 0, use_graph: bool = True):
         """Trains on the (X, Y) pairs (lists of arrays or tensors); targets are standardised
         with their global mean / std, which transform() undoes.  With ``use_graph`` the
-        training step (batch gather, forward, backward, AdamW) is recorded once into a
+        training step (row gather, forward, backward, AdamW) is recorded once into a
         CUDA graph and replayed for every batch after the first."""
         Xd = torch.cat([to_device_f32(x, self.dev) for x in Xs])
         Yd = torch.cat([to_device_f32(y, self.dev) for y in Ys])
@@ -190,7 +209,7 @@ class Encoder:
         total = torch.zeros((), device=self.dev)
 
         def step():
-            loss = self.train_step(torch.index_select(Xd, 0, sel), torch.index_select(Yn, 0, sel))
+            loss = self.train_step(Xd, Yn, rows=sel)
             total.add_(loss[0])
 
         graph = None

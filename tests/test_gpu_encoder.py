@@ -16,20 +16,21 @@ def gemm(A, B, epi=0, bias=None, Z=None, with_t=False, ksplit=1, colsum=False):
     M, K = A.shape
     N = B.shape[0]
     st = torch.zeros(1, dtype=torch.int32, device="cuda")
-    C = torch.full((M, N), float("nan"), device="cuda") if epi == 0 else None
+    Cs = torch.full((ksplit, M, N), float("nan"), device="cuda") if epi == 0 else None  # K slices
     H = torch.empty((M, N), dtype=torch.bfloat16, device="cuda") if epi else None
     HT = torch.empty((N, M), dtype=torch.bfloat16, device="cuda") if (epi and with_t) else None
     Zo = torch.empty((M, N), device="cuda") if epi == 1 else Z
     cs = torch.full((N,), float("nan"), device="cuda") if colsum else None
     _lib.call("umapb_gemm_bf16", _lib.ptr(A), _lib.ptr(B), M, N, K, A.stride(0), B.stride(0), epi, ksplit,
-              _lib.ptr(C), N, _lib.ptr(bias), _lib.ptr(Zo), N, _lib.ptr(H), N, _lib.ptr(HT), M, _lib.ptr(cs),
+              _lib.ptr(Cs), N, _lib.ptr(bias), _lib.ptr(Zo), N, _lib.ptr(H), N, _lib.ptr(HT), M, _lib.ptr(cs),
               _lib.ptr(st), _lib.stream_handle())
     torch.cuda.synchronize()
     assert int(st.item()) == 0
+    C = Cs.sum(0) if Cs is not None else None
     return (C, Zo, H, HT, cs) if colsum else (C, Zo, H, HT)
 
 
-@pytest.mark.parametrize("ksplit", [1, 8])
+@pytest.mark.parametrize("ksplit", [1, 8, 48])
 @pytest.mark.parametrize("M,N,K", [(300, 200, 104), (4096, 512, 784), (512, 784, 4096), (128, 128, 64), (1, 8, 8),
                                    (512, 512, 4000)])
 def test_gemm_f32_matches_float64(M, N, K, ksplit):
