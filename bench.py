@@ -199,6 +199,18 @@ def run_ours(args, rank, world, local_rank):
     for m in models:
         m.profile_kernels = True
     barrier()
+    gc_pauses = []  # Python garbage-collector pauses inside the timed fits (ms)
+    gc_t = [0.0]
+
+    def gc_cb(phase, info):
+        if phase == "start":
+            gc_t[0] = time.perf_counter()
+        else:
+            gc_pauses.append((time.perf_counter() - gc_t[0]) * 1e3)
+
+    import gc
+
+    gc.callbacks.append(gc_cb)
     clk = Clocks(local_rank)
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
@@ -208,6 +220,7 @@ def run_ours(args, rank, world, local_rank):
     t1.record()
     barrier()
     clocks = clk.stop()
+    gc.callbacks.remove(gc_cb)
     launches = _lib.kernel_launches() - launches0
     ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
@@ -215,6 +228,7 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
 
+    gc_ms = [round(x, 2) for x in gc_pauses]
     fit_ms_each = [round(m.timings_["total_device"], 2) for m in models]
     stage_ms_each = [{k: round(v, 2) for k, v in m.timings_.items()} for m in models]
     # roofline of the NNDescent iteration kernel from the events of the timed fits
@@ -268,7 +282,7 @@ def run_ours(args, rank, world, local_rank):
                "config": config(n),
                "edges_per_fit": edges_per_fit, "n_edges_graph": E,
                "stage_ms": {k: round(v, 2) for k, v in stages.items()}, "fit_ms_each": fit_ms_each,
-               "stage_ms_each": stage_ms_each,
+               "stage_ms_each": stage_ms_each, "gc_pause_ms": gc_ms,
                "layout_edges_per_s": edges_per_fit / (stages["layout"] * 1e-3),
                "roofline": roofline,
                "e2e": {"value": edges_per_fit * world / (e2e_ms * 1e-3), "unit": "edges/s", "fit_s": round(e2e_ms * 1e-3, 4),

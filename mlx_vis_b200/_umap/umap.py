@@ -10,16 +10,19 @@ and after every epoch that has active edges (umap.py:420-442).
 Pipeline, all on the GPU through libumap_b200:
   kNN (brute tcgen05 / NNDescent) -> fuzzy set (FP64 sigma bisection)
   -> spectral init (CSR SpMV + Cholesky-QR power iteration)
-  -> layout epochs (exact float32 schedule, synchronous SGD), by default
-     recorded once into a CUDA graph and replayed.
-Host work left: the a/b curve fit (float64, microseconds) and the reference's
-NumPy noise draw for the spectral rescale (umap.py:344).
+  -> layout epochs (exact float32 schedule, synchronous SGD), two launches per
+     epoch issued by the library (optionally recorded into a CUDA graph).
+Host work left: the a/b curve fit (float64, microseconds); the NumPy streams the
+reference draws from are seeded on the host and drawn on the device.
 
 New keyword arguments (defaults keep the reference behaviour):
   init        "spectral" (reference), "random" (N(0, 1e-4) like the reference's
               fallback), or "learned" (the MLP warm start of ``encoder``)
   encoder     a trained ``mlx_vis_b200.encoder.Encoder`` for init="learned"
-  use_graph   capture the epoch loop in a CUDA graph (no callback only)
+  use_graph   capture the epoch loop in a CUDA graph (no callback only).  Off by
+              default: the 2 x n_epochs launches are issued straight from the
+              library, which costs about 1 ms of device gaps per 500 epochs,
+              while a per-fit capture costs host milliseconds (at times tens).
 """
 
 from __future__ import annotations
@@ -64,7 +67,7 @@ class UMAP:
         normalize: str | bool = False,
         init: str = "spectral",
         encoder=None,
-        use_graph: bool = True,
+        use_graph: bool = False,
     ):
         self.n_components = n_components
         self.n_neighbors = n_neighbors

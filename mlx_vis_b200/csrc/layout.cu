@@ -150,6 +150,32 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
                                             uint32_t k1) {
   const int i = rows[e], j = cols[e];
   float yi[DIM], yj[DIM], acc[DIM], pos[DIM], neg_pos[DIM];
+  if (neg_rate <= 8) {
+    // up to 8 negatives: draw their tails and issue every gather of Y before the
+    // arithmetic, so the seven or so random reads of an edge are in flight together
+    const U4 r0 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 0u}, k0, k1);
+    U4 r1 = r0;
+    if (neg_rate > 4) r1 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 1u}, k0, k1);
+    const uint32_t rr[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
+    float yt[8][DIM];
+    load_row<DIM>(Y, i, yi);
+    load_row<DIM>(Y, j, yj);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (u < neg_rate) load_row<DIM>(Y, to_range(rr[u], (uint32_t)n), yt[u]);
+    attract<DIM>(yi, yj, p, pos);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      acc[c] = pos[c];
+      neg_pos[c] = -pos[c];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (u < neg_rate) repel_add<DIM>(yi, yt[u], p, acc);
+    atomic_add_row<DIM>(dY, j, neg_pos);
+    atomic_add_row<DIM>(dY, i, acc);
+    return;
+  }
   load_row<DIM>(Y, i, yi);
   load_row<DIM>(Y, j, yj);
   attract<DIM>(yi, yj, p, pos);

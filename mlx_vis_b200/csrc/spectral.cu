@@ -7,7 +7,8 @@
 // min-max each column to [0, 10].
 //
 // Here the edges are in row-major order, so W V is a CSR SpMV without atomics
-// (8 lanes per row, FP64 partial sums combined by shuffles).  MGS of the
+// (8 lanes per row, FP64 partial sums combined by shuffles; V kept in FP32 rows
+// padded to 16 bytes, one vector load per edge, Gram matrix and R^-1 in FP64).  MGS of the
 // (c+1)-column block equals Q = V R^-1 with R the Cholesky factor of the Gram
 // matrix V^T V (+1e-10 on each pivot, as in the reference's norms), so each
 // iteration is ONE kernel: it applies the previous iteration's R^-1 to every
@@ -89,9 +90,9 @@ __device__ void chol_inverse(const double* G, int kk, double* ri) {
 // few edges to hundreds) and meet by shuffles.  The last block to finish (a counter
 // per iteration) factors the completed G_out once and writes Rinv_out for the next
 // iteration.
-__global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* __restrict__ Rinv_in,
+__global__ void spmv_gram_kernel(const float* __restrict__ Vin, const double* __restrict__ Rinv_in,
                                  const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ cols,
-                                 const float* __restrict__ wn, int64_t n, int kk, double* __restrict__ Vout,
+                                 const float* __restrict__ wn, int64_t n, int kk, int vp, float* __restrict__ Vout,
                                  double* __restrict__ G_out, unsigned* __restrict__ counter,
                                  double* __restrict__ Rinv_out) {
   __shared__ double ri[kMaxCols * kMaxCols];
@@ -109,7 +110,9 @@ __global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* _
       const int64_t c = cols[e];
       const double w = (double)wn[e];
       double v[kMaxCols];
-      for (int j = 0; j < kk; ++j) v[j] = Vin[c * kk + j];
+      const float4 a = reinterpret_cast<const float4*>(Vin + c * vp)[0];  // rows padded to 4 or 8 floats
+      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+      if (kk > 4) v[4] = Vin[c * vp + 4];
       for (int j = 0; j < kk; ++j) {  // q_j = sum_i v_i Rinv[i][j]
         double q = 0.0;
         for (int i = 0; i <= j; ++i) q += v[i] * ri[i * kk + j];
@@ -122,7 +125,7 @@ __global__ void spmv_gram_kernel(const double* __restrict__ Vin, const double* _
     for (int o = kLanes / 2; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
   }
   if (r < n && sub == 0)
-    for (int j = 0; j < kk; ++j) Vout[r * kk + j] = acc[j];
+    for (int j = 0; j < vp; ++j) Vout[r * vp + j] = j < kk ? (float)acc[j] : 0.f;
   if (sub != 0)
     for (int j = 0; j < kk; ++j) acc[j] = 0.0;  // one copy of each row in the Gram sum
   // block reduction of the Gram matrix
@@ -166,8 +169,8 @@ __device__ __forceinline__ float ord2f(unsigned u) {
 }
 
 // embedding = (V R^-1)[:, 1:], max |embedding|
-__global__ void finish_orth_kernel(const double* __restrict__ V, const double* __restrict__ Rinv, int64_t n, int kk,
-                                   float* __restrict__ emb, unsigned* __restrict__ absmax) {
+__global__ void finish_orth_kernel(const float* __restrict__ V, const double* __restrict__ Rinv, int64_t n, int kk,
+                                   int vp, float* __restrict__ emb, unsigned* __restrict__ absmax) {
   __shared__ double ri[kMaxCols * kMaxCols];
   if (threadIdx.x < kk * kk) ri[threadIdx.x] = Rinv[threadIdx.x];
   __syncthreads();
@@ -176,7 +179,7 @@ __global__ void finish_orth_kernel(const double* __restrict__ V, const double* _
   if (r < n) {
     for (int j = 1; j < kk; ++j) {
       double q = 0.0;
-      for (int i = 0; i <= j; ++i) q += V[r * kk + i] * ri[i * kk + j];
+      for (int i = 0; i <= j; ++i) q += (double)V[r * vp + i] * ri[i * kk + j];
       const float f = (float)q;
       emb[r * (kk - 1) + (j - 1)] = f;
       m = fmaxf(m, fabsf(f));
@@ -219,7 +222,7 @@ struct Layout {
   int64_t* row_ptr;
   float* dis;
   float* wn;
-  double* V[2];
+  float* V[2];  // n rows of vp floats (kk values, zero padded to 4 or 8)
   double* G;       // n_iter blocks of kk*kk
   double* Rinv;    // n_iter blocks of kk*kk: the inverse Cholesky factor after each iteration
   unsigned* done;  // per-iteration block counters
@@ -227,6 +230,8 @@ struct Layout {
   unsigned* red;  // absmax, colmin[4], colmax[4]
   size_t bytes;
 };
+
+static int vpitch(int kk) { return kk <= 4 ? 4 : 8; }
 
 static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   const int kk = dim + 1;
@@ -236,8 +241,8 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   l.row_ptr = c.take<int64_t>((size_t)n + 1);
   l.dis = c.take<float>((size_t)n);
   l.wn = c.take<float>((size_t)(e_cap > 0 ? e_cap : 1));
-  l.V[0] = c.take<double>((size_t)n * kk);
-  l.V[1] = c.take<double>((size_t)n * kk);
+  l.V[0] = c.take<float>((size_t)n * vpitch(kk));
+  l.V[1] = c.take<float>((size_t)n * vpitch(kk));
   l.G = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
   l.Rinv = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
   l.done = c.take<unsigned>((size_t)(n_iter > 0 ? n_iter : 1));
@@ -247,9 +252,13 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   return l;
 }
 
-__global__ void f32_to_f64_kernel(const float* __restrict__ a, double* __restrict__ b, int64_t m) {
+// V0 (n x kk) into rows of vp floats, zero padded
+__global__ void pad_rows_kernel(const float* __restrict__ a, int64_t n, int kk, int vp, float* __restrict__ b) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < m) b[t] = (double)a[t];
+  if (t >= n * vp) return;
+  const int64_t r = t / vp;
+  const int j = (int)(t - r * vp);
+  b[t] = j < kk ? a[r * kk + j] : 0.f;
 }
 
 // Standard normal draws: element i of the stream (seed) comes from Philox block i/4
@@ -316,21 +325,22 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   if (e_cap > 0)
     spectral::norm_weight_kernel<<<(unsigned)ceil_div(e_cap, spectral::kBlock), spectral::kBlock, 0, stream>>>(
         rows, cols, vals, n_edges, l.dis, l.wn);
-  spectral::f32_to_f64_kernel<<<(unsigned)ceil_div(n * kk, spectral::kBlock), spectral::kBlock, 0, stream>>>(
-      V0, l.V[0], n * kk);
+  const int vp = spectral::vpitch(kk);
+  spectral::pad_rows_kernel<<<(unsigned)ceil_div(n * vp, spectral::kBlock), spectral::kBlock, 0, stream>>>(
+      V0, n, kk, vp, l.V[0]);
   UMAPB_LAUNCH_CHECK("spectral: setup kernels");
   const unsigned pb = (unsigned)ceil_div(n * spectral::kLanes, spectral::kBlock);
   for (int it = 0; it < n_iter; ++it) {
     const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
     spectral::spmv_gram_kernel<<<pb, spectral::kBlock, 0, stream>>>(
-        l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk, l.done + it,
+        l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, vp, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk, l.done + it,
         l.Rinv + (size_t)it * kk * kk);
   }
   UMAPB_LAUNCH_CHECK("spectral: power iteration");
   spectral::init_red_kernel<<<1, 32, 0, stream>>>(l.red, dim);
   spectral::finish_orth_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[n_iter & 1],
                                                                      l.Rinv + (size_t)(n_iter - 1) * kk * kk, n,
-                                                                     kk, l.emb, l.red);
+                                                                     kk, vp, l.emb, l.red);
   const unsigned eb = (unsigned)ceil_div(n * dim, spectral::kBlock);
   spectral::scale_noise_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, noise, n, dim, l.red, l.red + 1,
                                                                      l.red + 5);
