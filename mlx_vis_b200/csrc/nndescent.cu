@@ -207,6 +207,18 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
   if (j >= n) return;
   const int cnt = deg[j];
   const int32_t* b = bucket + off[j];
+  if (cnt <= 32 && k <= 32) {  // the common case (mean in-degree k): one warp-wide bitonic sort
+    int v = lane < cnt ? b[lane] : 0x7fffffff;
+    for (int size = 2; size <= 32; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const int o = __shfl_xor_sync(0xffffffffu, v, stride);
+        const bool lower = (lane & stride) == 0, asc = (lane & size) == 0;
+        v = (lower == asc) ? min(v, o) : max(v, o);
+      }
+    }
+    if (lane < k) rev[j * k + lane] = lane < cnt ? v : 0;  // lane p holds the p-th smallest
+    return;
+  }
   // The sorted multiset of j's sources, first k of it: each pass emits the previous
   // source again while it has unused copies (a row that lists j twice), else the
   // next larger source; once the bucket is exhausted the remaining slots stay 0,

@@ -7,7 +7,7 @@
 // min-max each column to [0, 10].
 //
 // Here the edges are in row-major order, so W V is a CSR SpMV without atomics
-// (8 lanes per row, FP64 partial sums combined by shuffles; V kept in FP32 rows
+// (2 lanes per row, FP64 partial sums combined by shuffles; V kept in FP32 rows
 // padded to 16 bytes, one vector load per edge, Gram matrix and R^-1 in FP64).  MGS of the
 // (c+1)-column block equals Q = V R^-1 with R the Cholesky factor of the Gram
 // matrix V^T V (+1e-10 on each pivot, as in the reference's norms), so each
@@ -24,7 +24,7 @@ namespace spectral {
 
 constexpr int kBlock = 256;
 constexpr int kMaxCols = 5;  // n_components <= 4
-constexpr int kLanes = 8;    // lanes per row in the power iteration
+constexpr int kLanes = 2;    // lanes per row in the power iteration
 
 __global__ void row_ptr_kernel(const int32_t* __restrict__ rows, const int64_t* __restrict__ n_edges, int64_t n,
                                int64_t* __restrict__ row_ptr) {
