@@ -92,26 +92,76 @@ def schedule_edge_updates(vals: np.ndarray, n_epochs: int) -> int:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every 10 ms through NVML while the
+    timed region runs (the device is matched to the CUDA device by PCI bus id);
+    nvidia-smi at 200 ms when NVML is unavailable."""
+
+    NAMES = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4,
+             "hw_power_brake_slowdown": 0x80}
+
+    def __init__(self, index):
+        import threading
+
+        self.sm, self.smax, self.reasons, self.power = [], [], set(), []
+        self.stop_evt = threading.Event()
+        self.thread = None
+        self.smi = None
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(index)
+            try:
+                bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.smax.append(float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)))
+
+            def poll():
+                while not self.stop_evt.is_set():
+                    try:
+                        self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                        bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        for nm, b in self.NAMES.items():
+                            if bits & b:
+                                self.reasons.add(nm)
+                        self.power.append(pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0)
+                    except Exception:
+                        pass
+                    self.stop_evt.wait(0.01)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self._start_smi(index)
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
+    def _start_smi(self, index):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            self.smi = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}",
+                                         "--format=csv,noheader", "-lms", "200"], stdout=self.f,
+                                        stderr=subprocess.DEVNULL)
         except Exception:
-            self.p = None
+            self.smi = None
 
     def stop(self):
-        if self.p is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.p.terminate()
-        self.p.wait(timeout=10)
+        if self.thread is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None,
+                    "sm_max_mhz": max(self.smax) if self.smax else None, "reasons": sorted(self.reasons),
+                    "samples": len(self.sm), "power_w_max": max(self.power) if self.power else None,
+                    "source": "nvml, 10 ms"}
+        if self.smi is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.smi.terminate()
+        self.smi.wait(timeout=10)
         self.f.seek(0)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -129,7 +179,7 @@ class Clocks:
                     reasons.add(nm)
         os.unlink(self.f.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks():
