@@ -210,6 +210,16 @@ int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, c
                         int32_t epoch_end, int32_t n_epochs, float a, float b, float learning_rate,
                         int32_t neg_rate, uint64_t seed, void* workspace, size_t workspace_bytes,
                         umapb_stream_t stream);
+/* umapb_layout_epochs_graph: the same epochs, recorded into a CUDA graph and
+ * launched as one unit; the executable graph is cached per device and updated
+ * in place on later calls (same epoch count -> same topology), so the per-call
+ * host cost is the recording, not an instantiation.  The stream must not be under
+ * capture already. */
+int umapb_layout_epochs_graph(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                        const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int32_t epoch_begin,
+                        int32_t epoch_end, int32_t n_epochs, float a, float b, float learning_rate,
+                        int32_t neg_rate, uint64_t seed, void* workspace, size_t workspace_bytes,
+                        umapb_stream_t stream);
 /* Number of edges active in `epoch` given the current `next` values (written to
  * the device int64 *count) — the emptiness test of umap.py:409-414/424 that
  * decides whether the reference runs an epoch and calls epoch_callback.  Uses

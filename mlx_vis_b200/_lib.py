@@ -39,6 +39,8 @@ SIGNATURES = {
     "umapb_layout_prepare": [_p, _p, _i64, _i32, _p, _p, _p, _sz, _p],
     "umapb_layout_epochs": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32,
                             _u64, _p, _sz, _p],
+    "umapb_layout_epochs_graph": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32,
+                                  _i32, _u64, _p, _sz, _p],
     "umapb_nnd_sqnorms": [_p, _i64, _i32, _i32, _p, _p],
     "umapb_nnd_to_half": [_p, _i64, _i32, _i32, _p, _p],
     "umapb_nnd_gather": [_p, _p, _i64, _i32, _p, _p, _i32, _i32, _p],
@@ -240,8 +242,10 @@ class Layout:
              ptr(self.next), ptr(self.ws), self.ws.numel(), stream_handle())
 
     def epochs(self, Y: torch.Tensor, begin: int, end: int, a: float, b: float, learning_rate: float,
-               neg_rate: int, seed: int):
-        call("umapb_layout_epochs", ptr(Y), self.n, self.dim, ptr(self.rows), ptr(self.cols), ptr(self.eps),
+               neg_rate: int, seed: int, graph: bool = False):
+        """Runs epochs [begin, end); with ``graph`` as one cached, updated CUDA graph."""
+        call("umapb_layout_epochs_graph" if graph else "umapb_layout_epochs", ptr(Y), self.n, self.dim,
+             ptr(self.rows), ptr(self.cols), ptr(self.eps),
              ptr(self.next), ptr(self.n_edges), self.e_cap, int(begin), int(end), self.n_epochs, float(a), float(b),
              float(learning_rate), int(neg_rate), int(seed) & 0xFFFFFFFFFFFFFFFF, ptr(self.ws), self.ws.numel(),
              stream_handle())

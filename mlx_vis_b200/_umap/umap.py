@@ -11,7 +11,7 @@ Pipeline, all on the GPU through libumap_b200:
   kNN (brute tcgen05 / NNDescent) -> fuzzy set (FP64 sigma bisection)
   -> spectral init (CSR SpMV + Cholesky-QR power iteration)
   -> layout epochs (exact float32 schedule, synchronous SGD), two launches per
-     epoch issued by the library (optionally recorded into a CUDA graph).
+     epoch, run as one CUDA graph that the library records and updates per fit.
 Host work left: the a/b curve fit (float64, microseconds); the NumPy streams the
 reference draws from are seeded on the host and drawn on the device.
 
@@ -19,10 +19,10 @@ New keyword arguments (defaults keep the reference behaviour):
   init        "spectral" (reference), "random" (N(0, 1e-4) like the reference's
               fallback), or "learned" (the MLP warm start of ``encoder``)
   encoder     a trained ``mlx_vis_b200.encoder.Encoder`` for init="learned"
-  use_graph   capture the epoch loop in a CUDA graph (no callback only).  Off by
-              default: the 2 x n_epochs launches are issued straight from the
-              library, which costs about 1 ms of device gaps per 500 epochs,
-              while a per-fit capture costs host milliseconds (at times tens).
+  use_graph   run the epoch loop as one CUDA graph (no callback only; default).
+              The library records it and keeps one executable graph per device,
+              updated in place by later fits; False issues the 2 x n_epochs
+              launches one by one.
 """
 
 from __future__ import annotations
@@ -67,7 +67,7 @@ class UMAP:
         normalize: str | bool = False,
         init: str = "spectral",
         encoder=None,
-        use_graph: bool = False,
+        use_graph: bool = True,
     ):
         self.n_components = n_components
         self.n_neighbors = n_neighbors
@@ -86,7 +86,6 @@ class UMAP:
         self.use_graph = use_graph
         self.embedding_ = None
         self.timings_ = {}
-        self.graph_ = None
         self.profile_kernels = False  # CUDA events around NNDescent iteration kernels (bench roofline)
 
     # ------------------------------------------------------------------
@@ -151,7 +150,6 @@ class UMAP:
         self._optimize(rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback)
         ev.mark("layout")
         self.timings_ = ev.finish()
-        self.graph_ = None  # the replay has finished; release the graph and its memory pool
         self.graph_info_ = {"n_edges": int(n_edges.item())}
         return Y
 
@@ -209,19 +207,9 @@ class UMAP:
                 if self.verbose and (e + 1) % 50 == 0:
                     print(f"Epoch {e + 1}/{ne}")
             return
-        if self.use_graph and ne > 0:
-            g = torch.cuda.CUDAGraph()
-            s = torch.cuda.Stream()
-            s.wait_stream(torch.cuda.current_stream())
-            with torch.cuda.stream(s):
-                g.capture_begin()
-                lay.epochs(Y, 0, ne, *args)
-                g.capture_end()
-            torch.cuda.current_stream().wait_stream(s)
-            g.replay()
-            self.graph_ = g  # keep the graph alive until its work has finished
-        else:
-            lay.epochs(Y, 0, ne, *args)
+        # by default the whole epoch loop is one CUDA graph, recorded by the library and
+        # kept per device (later fits only update its parameters)
+        lay.epochs(Y, 0, ne, *args, graph=self.use_graph and ne > 0)
         if self.verbose:
             print(f"Epoch {ne}/{ne}")
 

@@ -25,6 +25,8 @@
 // for the r-th active edge.
 #include <math.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "philox.cuh"
 #include "scan.cuh"
@@ -429,13 +431,11 @@ extern "C" int umapb_layout_prepare(const float* vals, const int64_t* n_edges, i
   return UMAPB_OK;
 }
 
-extern "C" int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
-                                   const float* eps, float* next, const int64_t* n_edges, int64_t e_cap,
-                                   int32_t epoch_begin, int32_t epoch_end, int32_t n_epochs, float a, float b,
-                                   float learning_rate, int32_t neg_rate, uint64_t seed, void* workspace,
-                                   size_t workspace_bytes, umapb_stream_t stream_) {
-  clear_error();
-  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+static int enqueue_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                          const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int32_t epoch_begin,
+                          int32_t epoch_end, int32_t n_epochs, float a, float b, float learning_rate,
+                          int32_t neg_rate, uint64_t seed, void* workspace, size_t workspace_bytes,
+                          cudaStream_t stream) {
   UMAPB_REQUIRE(Y && rows && cols && eps && next && n_edges, "layout_epochs: null array argument");
   UMAPB_REQUIRE(n >= 1 && n < ((int64_t)1 << 31), "layout_epochs: need 1 <= n < 2^31");
   UMAPB_REQUIRE(dim >= 1 && dim <= 4, "layout_epochs: dim must be in [1, 4]");
@@ -458,6 +458,76 @@ extern "C" int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32
   }
   UMAPB_LAUNCH_CHECK("layout_epochs kernels");
   count_launches(2 * (epoch_end - epoch_begin));
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_layout_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows, const int32_t* cols,
+                                   const float* eps, float* next, const int64_t* n_edges, int64_t e_cap,
+                                   int32_t epoch_begin, int32_t epoch_end, int32_t n_epochs, float a, float b,
+                                   float learning_rate, int32_t neg_rate, uint64_t seed, void* workspace,
+                                   size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  return enqueue_epochs(Y, n, dim, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, n_epochs, a, b,
+                        learning_rate, neg_rate, seed, workspace, workspace_bytes,
+                        reinterpret_cast<cudaStream_t>(stream_));
+}
+
+// One executable graph per device, reused across calls: each call records its
+// launches (stream capture, thread-local mode, on a private non-blocking stream:
+// the caller's stream may be the legacy default stream, which cannot be captured),
+// updates the cached executable with the new parameters (cudaGraphExecUpdate; same
+// topology for the same epoch count) or instantiates a new one, and launches it on
+// the caller's stream.  Updates affect later launches only, so a replay still in
+// flight keeps its parameters.
+namespace {
+std::mutex g_graph_mu;
+cudaGraphExec_t g_graph_exec[64] = {};
+cudaStream_t g_capture_stream[64] = {};
+}  // namespace
+
+extern "C" int umapb_layout_epochs_graph(float* Y, int64_t n, int32_t dim, const int32_t* rows,
+                                         const int32_t* cols, const float* eps, float* next, const int64_t* n_edges,
+                                         int64_t e_cap, int32_t epoch_begin, int32_t epoch_end, int32_t n_epochs,
+                                         float a, float b, float learning_rate, int32_t neg_rate, uint64_t seed,
+                                         void* workspace, size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  int dev = 0;
+  UMAPB_CUDA_TRY(cudaGetDevice(&dev), "layout_epochs_graph: device");
+  UMAPB_REQUIRE(dev >= 0 && dev < 64, "layout_epochs_graph: device index out of range");
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  UMAPB_CUDA_TRY(cudaStreamIsCapturing(stream, &cs), "layout_epochs_graph: capture query");
+  UMAPB_REQUIRE(cs == cudaStreamCaptureStatusNone, "layout_epochs_graph: the stream is already being captured");
+  std::lock_guard<std::mutex> lock(g_graph_mu);
+  cudaStream_t& cap = g_capture_stream[dev];
+  if (!cap) UMAPB_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "layout_epochs_graph: stream");
+  UMAPB_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "layout_epochs_graph: capture");
+  const int rc = enqueue_epochs(Y, n, dim, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, n_epochs, a,
+                                b, learning_rate, neg_rate, seed, workspace, workspace_bytes, cap);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+  if (rc != UMAPB_OK || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != UMAPB_OK) return rc;
+    return set_error(UMAPB_ERR_CUDA, "layout_epochs_graph: end of capture: %s", cudaGetErrorString(ce));
+  }
+  cudaGraphExec_t& exec = g_graph_exec[dev];
+  if (exec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(exec, graph, &info) != cudaSuccess) {
+      cudaGetLastError();  // a topology change: instantiate anew
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (!exec) e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    exec = nullptr;
+    return set_error(UMAPB_ERR_CUDA, "layout_epochs_graph: instantiate: %s", cudaGetErrorString(e));
+  }
+  UMAPB_CUDA_TRY(cudaGraphLaunch(exec, stream), "layout_epochs_graph: launch");
   return UMAPB_OK;
 }
 

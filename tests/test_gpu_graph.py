@@ -143,3 +143,22 @@ def test_device_legacy_normal_equals_numpy(seed, shape, parallel):
     want = np.random.RandomState(seed).normal(scale=0.0001, size=shape).astype(np.float32)
     got = _lib.legacy_normal(np.random.RandomState(seed), shape, 0.0, 0.0001, torch.device("cuda"), parallel=parallel)
     assert np.array_equal(got.cpu().numpy(), want)
+
+
+def test_graph_epochs_match_launched_epochs(golden, manifest):
+    """umapb_layout_epochs_graph (recorded once, then updated in place for a new
+    layout) reaches the same coordinates as the launch-by-launch loop; float atomics
+    may add the moves of one point in another order, hence the tolerance."""
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    outs = []
+    for graph in (False, True, True):  # the second graph call updates the cached executable
+        lay = _layout(fz)
+        Y = cuda(opt["Y_ep0"].copy())
+        lay.epochs(Y, 0, 6, m["a"], m["b"], 1.0, 5, 7, graph=graph)
+        outs.append(Y.cpu().numpy())
+    scale = float(np.abs(outs[0]).max())
+    assert np.abs(outs[0] - opt["Y_ep0"]).max() > 1e-3 * scale  # the epochs moved the points
+    for o in outs[1:]:
+        assert np.median(np.abs(o - outs[0])) < 1e-5 * scale
+        assert np.abs(o - outs[0]).max() < 1e-2 * scale
