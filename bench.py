@@ -52,9 +52,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_FULL, help="rows (default: the 70K workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["fit", "learned_init", "nndescent", "knn_brute", "layout", "encoder"],
-                    default="fit",
+    ap.add_argument("--case", choices=["fit", "learned_init", "scale", "nndescent", "knn_brute", "layout",
+                                       "encoder"], default="fit",
                     help="fit: the benchmark line; learned_init: epochs-to-trustworthiness of the learned warm start; "
+                         "scale: the 1,000,000 x 128 configuration (plain fit, learned vs plain init); "
                          "nndescent / knn_brute / layout: one untimed run of that stage (profiler captures)")
     return ap.parse_args()
 
@@ -441,6 +442,57 @@ def run_learned_init(args):
             "unseen_prototypes": fresh}
 
 
+def run_scale(args):
+    """1,000,000 x 128 mixture of 100 anisotropic Gaussians (shared cluster parameters,
+    param_seed 0): plain UMAP (NNDescent k=15, 200 epochs) timed per stage, then an
+    encoder 128 -> 512 -> 512 -> 2 trained on 4 draws of 250,000 rows of the same
+    distribution, learned against spectral init; trustworthiness@15 on a fixed
+    20,000-row sample."""
+    import torch
+
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import anisotropic_mixture
+    from mlx_vis_b200.encoder import Encoder
+    from mlx_vis_b200.metrics import trustworthiness
+
+    n, d = 1_000_000, 128
+    X = anisotropic_mixture(n, d, 100, seed=0, param_seed=0)
+    Xd = torch.from_numpy(X).cuda()
+    sub = np.random.default_rng(0).choice(n, 20000, replace=False)
+
+    def fit(init, ne, enc=None):
+        u = UMAP(n_epochs=ne, random_state=0, knn_method="nndescent", init=init, encoder=enc)
+        Y = u.fit_transform_device(Xd)
+        return u, Y.cpu().numpy()
+
+    fit("spectral", 200)  # warm-up
+    fits = [fit("spectral", 200) for _ in range(3)]
+    u, Y = fits[-1]
+    plain = {"fit_s": [round(f[0].timings_["total_device"] * 1e-3, 4) for f in fits],
+             "stage_ms": {k: round(v, 2) for k, v in u.timings_.items() if not k.startswith("host_")},
+             "n_edges": u.graph_info_["n_edges"], "trust": round(trustworthiness(X[sub], Y[sub], 15), 5)}
+    t0 = time.perf_counter()
+    Xs = [anisotropic_mixture(250_000, d, 100, seed=j, param_seed=0) for j in range(1, 5)]
+    enc = Encoder.train_on_umap_runs(Xs, n_epochs=200, encoder_epochs=20, seed=0)
+    train_s = time.perf_counter() - t0
+    curves = {}
+    for init in ("spectral", "learned"):
+        curves[init] = {}
+        for ne in (25, 50, 100, 200):
+            uu, YY = fit(init, ne, enc)
+            curves[init][ne] = {"trust": round(trustworthiness(X[sub], YY[sub], 15), 5),
+                                "fit_ms": round(uu.timings_["total_device"], 1)}
+    ref = curves["spectral"][200]["trust"]
+    first = {str(tol): next((ne for ne in (25, 50, 100, 200) if curves["learned"][ne]["trust"] >= ref - tol), None)
+             for tol in (0.005, 0.001)}
+    return {"case": "scale", "config": {"workload": "UMAP fit_transform of a 1000000x128 mixture of 100 anisotropic "
+                                                    "Gaussians (Dirichlet(2) sizes); NNDescent k=15, 200 epochs",
+                                        "trust_sample": 20000},
+            "plain": plain, "encoder_train_s": round(train_s, 2), "curves": curves,
+            "learned_epochs_to_within": first, "transform_only_trust":
+                round(trustworthiness(X[sub], enc.transform(X[sub]), 15), 5)}
+
+
 def run_stage(args):
     """One untimed run of a single stage on its benchmark size, for profiler captures."""
     import torch
@@ -509,6 +561,8 @@ def main():
         out = run_reference(args, rank)
     elif args.case == "learned_init":
         out = run_learned_init(args) if rank == 0 else None
+    elif args.case == "scale":
+        out = run_scale(args) if rank == 0 else None
     elif args.case != "fit":
         out = run_stage(args) if rank == 0 else None
     else:

@@ -66,20 +66,27 @@ def prototype_mixture(n: int = 20000, d: int = 784, n_classes: int = 10,
 
 
 def anisotropic_mixture(n: int = 1_000_000, d: int = 128, n_clusters: int = 100,
-                        center_std: float = 8.0, seed: int = 0, return_labels: bool = False):
-    """Rotated anisotropic Gaussian mixture with Dirichlet(2) cluster sizes."""
-    rng = np.random.default_rng(seed)
-    sizes = rng.dirichlet(np.full(n_clusters, 2.0))
+                        center_std: float = 8.0, seed: int = 0, param_seed: int | None = None,
+                        return_labels: bool = False):
+    """Rotated anisotropic Gaussian mixture: cluster sizes ~ Dirichlet(2), centres
+    ~ N(0, center_std^2 I), random orthogonal rotations, per-axis sigma ~ U(0.3, 2).
+
+    ``param_seed`` fixes the clusters (sizes, centres, rotations, scales; defaults to
+    ``seed``) and ``seed`` the sampled rows, so several draws can share one
+    distribution."""
+    prng = np.random.default_rng(seed if param_seed is None else param_seed)
+    sizes = prng.dirichlet(np.full(n_clusters, 2.0))
+    centers = (prng.standard_normal((n_clusters, d)) * center_std).astype(np.float32)
+    rots = [np.linalg.qr(prng.standard_normal((d, d)))[0].astype(np.float32) for _ in range(n_clusters)]
+    scales = prng.uniform(0.3, 2.0, (n_clusters, d)).astype(np.float32)
+    rng = np.random.default_rng((seed, 1))
     counts = np.floor(sizes * n).astype(np.int64)
     counts[: n - counts.sum()] += 1
     labels = np.repeat(np.arange(n_clusters, dtype=np.int32), counts)
     rng.shuffle(labels)
-    centers = rng.standard_normal((n_clusters, d)) * center_std
     X = np.empty((n, d), dtype=np.float32)
     for c in range(n_clusters):
         rows = np.nonzero(labels == c)[0]
-        q, _ = np.linalg.qr(rng.standard_normal((d, d)))
-        scales = rng.uniform(0.3, 2.0, d)
-        z = rng.standard_normal((rows.size, d)) * scales
-        X[rows] = (z @ q.T + centers[c]).astype(np.float32)
+        z = rng.standard_normal((rows.size, d), dtype=np.float32) * scales[c]
+        X[rows] = z @ rots[c].T + centers[c]
     return (X, labels) if return_labels else X
