@@ -97,7 +97,11 @@ int umapb_read_status(const void* workspace, umapb_stream_t stream) {
   UMAPB_CUDA_TRY(cudaMemcpyAsync(&st, workspace, sizeof(st), cudaMemcpyDeviceToHost, stream), "status readback");
   UMAPB_CUDA_TRY(cudaStreamSynchronize(stream), "status readback sync");
   if (st != 0)
-    return umapb::set_error(UMAPB_ERR_DEVICE, "device-side wait expired (code %d); results are invalid", int(st));
+    return umapb::set_error(UMAPB_ERR_DEVICE,
+                            st == umapb::kDevBadLaunch
+                                ? "kernel launched with a wrong shape did nothing (code %d); results are invalid"
+                                : "device-side wait expired (code %d); results are invalid",
+                            int(st));
   return UMAPB_OK;
 }
 

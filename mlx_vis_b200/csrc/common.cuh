@@ -66,6 +66,7 @@ enum DeviceStatus : int32_t {
   kDevTimeoutProducer = 1,
   kDevTimeoutMma = 2,
   kDevTimeoutEpilogue = 3,
+  kDevBadLaunch = 4,  // a kernel found its launch shape wrong and did nothing
 };
 
 }  // namespace umapb

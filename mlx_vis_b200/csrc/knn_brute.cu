@@ -8,19 +8,27 @@
 //            distance (|x~_i|^2 is constant along the row).  The three extra K
 //            columns live in padding the 64-wide K blocks carry anyway.
 // 2. topk:   persistent tcgen05 kernel.  The n x n score matrix is cut into
-//            128 x 256 tiles (query rows x points); CTA c owns the contiguous
-//            tile range [c*T/G, (c+1)*T/G) in (row block, column tile) order.
-//            warp 0 streams A/B k-blocks with TMA (128-byte swizzle, zero fill
-//            past n and d), warp 1 issues tcgen05.mma into one of two TMEM
-//            accumulators (2 x 256 columns), warps 4-7 read the finished
-//            accumulator (one TMEM lane = one query row per thread) and keep
-//            the row's best L scores.  When the CTA leaves a row block it writes
-//            the lists to cand[row][slot] (slot = which CTA of that row block).
+//            tiles of 256 points (MMA N) by 256 query rows (L <= 32: a CTA pair
+//            on one TPC, cluster of 2, tcgen05.mma.cta_group::2 with M = 256) or
+//            by 128 rows (L > 32, or pairing switched off: one CTA, M = 128);
+//            unit u (pair or CTA) owns the contiguous tile range
+//            [u*T/G, (u+1)*T/G) in (row block, column tile) order.  In every CTA
+//            warp 0 streams k-blocks with TMA (128-byte swizzle, zero fill past
+//            n and d): its own 128 query rows and, in a pair, its half (128) of
+//            the tile's points, so each CTA reads (128 + 128) x K per 128 x 256
+//            outputs instead of (128 + 256) x K.  Warp 1 of the even CTA issues
+//            the MMAs into one of two TMEM accumulators (2 x 256 columns, rows
+//            split over the pair's TMEMs), warps 4-7 of each CTA read the
+//            finished accumulator (one TMEM lane = one query row per thread) and
+//            keep the row's best L scores.  When a unit leaves a row block it
+//            writes the lists to cand[row][slot] (slot = which unit of that row
+//            block).
 // 3. rerank: one warp per row merges its slots, keeps the best L by
 //            (score, index), recomputes those L distances exactly in FP32
 //            (sum of (x_i - x_j)^2) and writes the k nearest by (distance, index).
 #include <cuda_bf16.h>
 #include <math.h>
+#include <stdlib.h>
 
 #include <mutex>
 #include <vector>
@@ -36,8 +44,6 @@ constexpr int BN = 256;  // points per tile = MMA N
 constexpr int BK = 64;   // BF16 elements per 128-byte swizzled row
 constexpr int UK = 16;   // K of one tcgen05.mma kind::f16
 constexpr int A_BYTES = BM * BK * 2;
-constexpr int B_BYTES = BN * BK * 2;
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int THREADS = 256;  // warp 0 TMA, warp 1 MMA, warp 2 TMEM owner, warps 4-7 epilogue
 
 constexpr int BUF = 48;        // per-row hit buffer (entries) of the batched selection
@@ -49,19 +55,27 @@ constexpr int STG_PITCH = 36;  // floats per staging row (32 scores + padding)
 // shared memory; batches of 16 are merged by data-independent sorting networks,
 // so the 32 rows of a warp merge in lockstep without divergence.
 // LCAP > 32: per-thread sorted lists in shared memory with insertion.
-template <int LCAP>
+// PAIR: the CTA holds 128 of the tile's 256 points (its half of the pair's B).
+template <int LCAP, bool PAIR>
 struct Cfg {
+  static_assert(!PAIR || LCAP == 32, "CTA pairs run the batched top-32 epilogue only");
   static constexpr bool kWarpSelect = LCAP == 32;
-  static constexpr int kStages = LCAP <= 32 ? 3 : (LCAP <= 64 ? 3 : 2);
+  static constexpr int kBBytes = (PAIR ? BN / 2 : BN) * BK * 2;
+  static constexpr int kStageBytes = A_BYTES + kBBytes;
+  static constexpr int kRowsPerBlock = PAIR ? 2 * BM : BM;
+  static constexpr int kStages = PAIR ? 4 : (LCAP <= 64 ? 3 : 2);
   static constexpr int kListBytes = kWarpSelect ? BM * BUF * 8 + BM * STG_PITCH * 4 : BM * LCAP * 8;
   static constexpr int kBarBytes = 256;
-  static constexpr int kSmem = 1024 + kStages * STAGE_BYTES + kListBytes + kBarBytes;
+  static constexpr int kSmem = 1024 + kStages * kStageBytes + kListBytes + kBarBytes;
 };
 
 struct Plan {
   int64_t n, d, ld;
   int k, L, lcap, num_kb, slots;
-  int64_t row_blocks, col_tiles, tiles, grid, cols_pad;
+  bool pair;     // 256-row tiles on CTA pairs (cta_group::2)
+  int rb_rows;   // query rows per row block: 256 (pair) or 128
+  int64_t row_blocks, col_tiles, tiles, cols_pad;
+  int64_t grid;  // work units: CTA pairs (pair) or CTAs
   size_t ws_bytes;
   // workspace layout
   int32_t* status;
@@ -72,8 +86,18 @@ struct Plan {
 };
 
 __host__ __device__ inline int64_t first_cta(int64_t tile, int64_t tiles, int64_t grid) {
-  // largest c with floor(c * tiles / grid) <= tile
+  // largest unit c with floor(c * tiles / grid) <= tile
   return ((tile + 1) * grid + tiles - 1) / tiles - 1;
+}
+
+// CTA pairs of the cluster launch that fit on the device at once (0: pairs
+// unavailable); defined after the kernel.
+static int64_t resident_pairs();
+
+// Pairing is on unless the environment sets UMAPB_KNN_PAIR=0 (read per call).
+static bool pairing_enabled() {
+  const char* e = getenv("UMAPB_KNN_PAIR");
+  return !(e && e[0] == '0' && e[1] == 0);
 }
 
 static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) {
@@ -94,11 +118,18 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) 
   // 128-byte TMA box row starts on a 128-byte boundary
   p.ld = (d + 3 + BK - 1) / BK * BK;
   p.num_kb = (int)ceil_div(p.ld, BK);
-  p.row_blocks = ceil_div(n, BM);
+  int64_t g = 0;
+  p.pair = false;
+  if (p.lcap == 32 && pairing_enabled()) {
+    g = resident_pairs();
+    p.pair = g > 0;
+  }
+  if (!p.pair) g = num_sms();
+  p.rb_rows = p.pair ? 2 * BM : BM;
+  p.row_blocks = ceil_div(n, p.rb_rows);
   p.col_tiles = ceil_div(n, BN);
   p.cols_pad = p.col_tiles * BN;
   p.tiles = p.row_blocks * p.col_tiles;
-  int64_t g = num_sms();
   p.grid = g < p.tiles ? g : p.tiles;
   int64_t slots = 1;
   for (int64_t rb = 0; rb < p.row_blocks; ++rb) {
@@ -207,12 +238,14 @@ __device__ __forceinline__ void merge_32_16(float (&lv)[32], int (&li)[32], cons
 
 
 // ---- 2. tcgen05 distance tiles + fused per-row top-L ------------------------
-template <int LCAP>
+template <int LCAP, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1)
     topk_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 int n, int num_kb, int64_t col_tiles, int64_t tiles, int slots,
                 int L, float* __restrict__ cand_s, int32_t* __restrict__ cand_i, int32_t* __restrict__ status) {
-  using C = Cfg<LCAP>;
+  using C = Cfg<LCAP, PAIR>;
+  constexpr int STAGE_BYTES = C::kStageBytes;
+  constexpr int RB = C::kRowsPerBlock;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* stages = smem;
@@ -226,10 +259,21 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
+  if constexpr (PAIR) {
+    uint32_t nrank;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(nrank));
+    if (nrank != 2) {  // cta_group::2 needs the cluster launch of two CTAs
+      if (threadIdx.x == 0) atomicExch(status, (int32_t)kDevBadLaunch);
+      return;
+    }
+  }
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int64_t G = gridDim.x;
-  const int64_t cta = blockIdx.x;
+  // rank 0 of a pair issues the MMAs and owns the full / tempty barriers the
+  // pair shares; rank 1 holds accumulator rows 128-255 of each tile
+  const uint32_t rank = PAIR ? tc::cluster_ctarank() : 0u;
+  const int64_t G = PAIR ? (int64_t)(gridDim.x >> 1) : (int64_t)gridDim.x;
+  const int64_t cta = PAIR ? (int64_t)(blockIdx.x >> 1) : (int64_t)blockIdx.x;  // work unit
   const int64_t t_begin = cta * tiles / G;
   const int64_t t_end = (cta + 1) * tiles / G;
 
@@ -240,7 +284,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       tc::mbar_init(&tfull[a], 1);
-      tc::mbar_init(&tempty[a], 128);
+      // pair: one arrival per epilogue warp of both CTAs
+      tc::mbar_init(&tempty[a], PAIR ? 8 : 128);
     }
     *abort_flag = 0;
     tc::fence_mbar_init();
@@ -249,7 +294,15 @@ __global__ void __launch_bounds__(THREADS, 1)
     tc::prefetch_tmap(&tmA);
     tc::prefetch_tmap(&tmB);
   }
-  if (warp == 2) tc::tmem_alloc(tmem_slot, 512);
+  if constexpr (PAIR) {
+    // both CTAs' barriers are initialised before any remote arrival or TMA
+    // completion reaches them; then the pair allocates TMEM together
+    __syncthreads();
+    tc::cluster_sync();
+    if (warp == 2) tc::tmem_alloc_pair(tmem_slot, 512);
+  } else {
+    if (warp == 2) tc::tmem_alloc(tmem_slot, 512);
+  }
   if (!C::kWarpSelect && warp >= 4) {
     const int r = threadIdx.x - 128;
     for (int e = 0; e < LCAP; ++e) {
@@ -263,7 +316,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t tmem_base = *tmem_slot;
 
   if (warp == 0) {
-    // ---------------- TMA producer ----------------
+    // ---------------- TMA producer (both CTAs of a pair) ----------------
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
@@ -273,9 +326,29 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int kb = 0; kb < num_kb; ++kb) {
           if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag)) goto producer_done;
           uint8_t* sa = stages + stage * STAGE_BYTES;
-          tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-          tc::tma_load_2d(sa, &tmA, &full[stage], kb * BK, rb * BM);
-          tc::tma_load_2d(sa + A_BYTES, &tmB, &full[stage], kb * BK, ct * BN);
+          if constexpr (PAIR) {
+            // both halves complete on rank 0's full barrier, which expects the
+            // bytes of both
+            const uint32_t fb = tc::mapa_shared(tc::smem_u32(&full[stage]), 0);
+            if (rank == 0) tc::mbar_arrive_expect_tx(&full[stage], 2 * STAGE_BYTES);
+            tc::tma_load_2d_pair(sa, &tmA, fb, kb * BK, rb * RB + (int)rank * BM);
+            tc::tma_load_2d_pair(sa + A_BYTES, &tmB, fb, kb * BK, ct * BN + (int)rank * (BN / 2));
+          } else {
+            tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+            tc::tma_load_2d(sa, &tmA, &full[stage], kb * BK, rb * BM);
+            tc::tma_load_2d(sa + A_BYTES, &tmB, &full[stage], kb * BK, ct * BN);
+          }
+          if (++stage == C::kStages) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+      if constexpr (PAIR) {
+        // every stage released once more: the last MMA commits have arrived on
+        // this CTA's empty barriers before it may exit
+        for (int i = 0; i < C::kStages; ++i) {
+          if (!tc::mbar_wait(&empty[stage], phase ^ 1, abort_flag)) break;
           if (++stage == C::kStages) {
             stage = 0;
             phase ^= 1;
@@ -285,18 +358,21 @@ __global__ void __launch_bounds__(THREADS, 1)
     producer_done:;
     }
   } else if (warp == 1) {
-    // ---------------- MMA issuer ----------------
-    if (lane == 0) {
-      constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+    // ---------------- MMA issuer (rank 0 of a pair) ----------------
+    if (lane == 0 && rank == 0) {
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(PAIR ? 2 * BM : BM, BN);
       int stage = 0;
       uint32_t phase = 0;
       int acc = 0;
       uint32_t acc_phase = 0;
+      bool ok = true;
       for (int64_t t = t_begin; t < t_end; ++t) {
-        if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag)) break;
+        if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag)) {
+          ok = false;
+          break;
+        }
         tc::tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-        bool ok = true;
         for (int kb = 0; kb < num_kb; ++kb) {
           if (!tc::mbar_wait(&full[stage], phase, abort_flag)) {
             ok = false;
@@ -307,19 +383,39 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t b_addr = a_addr + A_BYTES;
 #pragma unroll
           for (int k = 0; k < BK / UK; ++k) {
-            tc::mma_bf16(d_tmem, tc::sw128_kmajor_desc(a_addr + k * 32), tc::sw128_kmajor_desc(b_addr + k * 32),
-                         idesc, (kb | k) != 0 ? 1u : 0u);
+            const uint64_t ad = tc::sw128_kmajor_desc(a_addr + k * 32);
+            const uint64_t bd = tc::sw128_kmajor_desc(b_addr + k * 32);
+            const uint32_t accum = (kb | k) != 0 ? 1u : 0u;
+            if constexpr (PAIR)
+              tc::mma_bf16_pair(d_tmem, ad, bd, idesc, accum);
+            else
+              tc::mma_bf16(d_tmem, ad, bd, idesc, accum);
           }
-          tc::mma_commit(&empty[stage]);
+          if constexpr (PAIR)
+            tc::mma_commit_pair(&empty[stage], 0x3);
+          else
+            tc::mma_commit(&empty[stage]);
           if (++stage == C::kStages) {
             stage = 0;
             phase ^= 1;
           }
         }
         if (!ok) break;
-        tc::mma_commit(&tfull[acc]);
+        if constexpr (PAIR)
+          tc::mma_commit_pair(&tfull[acc], 0x3);
+        else
+          tc::mma_commit(&tfull[acc]);
         acc ^= 1;
         if (acc == 0) acc_phase ^= 1;
+      }
+      if (PAIR && ok) {
+        // both accumulators released by both CTAs' epilogues: no remote arrival
+        // is still on its way to this CTA when it exits
+        for (int i = 0; i < 2; ++i) {
+          if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, abort_flag)) break;
+          acc ^= 1;
+          if (acc == 0) acc_phase ^= 1;
+        }
       }
     }
   } else if (C::kWarpSelect && warp >= 4) {
@@ -373,7 +469,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     };
     auto flush = [&](int64_t rb) {
       merge_pending();
-      const int64_t row = rb * BM + r;
+      const int64_t row = rb * RB + (int64_t)rank * BM + r;
       const int64_t slot = cta - first_cta(rb * col_tiles, tiles, G);
       if (row < n) {
         float* cs = cand_s + (row * slots + slot) * L;
@@ -404,7 +500,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         break;
       }
       tc::tc_fence_after();
-      const int64_t row = rb * BM + r;
+      const int64_t row = rb * RB + (int64_t)rank * BM + r;
       const bool row_ok = row < n;
       const int self_col = row_ok ? (int)row : -1;
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
@@ -445,7 +541,13 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (__any_sync(0xffffffffu, cnt >= MERGE_AT)) merge_pending();
       }
       tc::tc_fence_before();
-      tc::mbar_arrive(&tempty[acc]);
+      if constexpr (PAIR) {
+        // one arrival per warp on rank 0's barrier, which counts both CTAs
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive_cluster(tc::mapa_shared(tc::smem_u32(&tempty[acc]), 0));
+      } else {
+        tc::mbar_arrive(&tempty[acc]);
+      }
       acc ^= 1;
       if (acc == 0) acc_phase ^= 1;
     }
@@ -526,7 +628,14 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 2) {
+  if constexpr (PAIR) {
+    // neither CTA frees the pair's TMEM or leaves while the other still works
+    tc::cluster_sync();
+    if (warp == 2) {
+      tc::tc_fence_after();
+      tc::tmem_dealloc_pair(tmem_base, 512);
+    }
+  } else if (warp == 2) {
     tc::tc_fence_after();
     tc::tmem_dealloc(tmem_base, 512);
   }
@@ -655,21 +764,97 @@ __global__ void __launch_bounds__(RR_WARPS * 32)
   }
 }
 
-template <int LCAP>
-static int launch_topk(const Plan& p, const CUtensorMap& ta, const CUtensorMap& tb, cudaStream_t stream) {
-  using C = Cfg<LCAP>;
+template <int LCAP, bool PAIR>
+static int set_smem_attr() {
+  using C = Cfg<LCAP, PAIR>;
   static bool attr_set[64] = {false};
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 64 && !attr_set[dev]) {
-    UMAPB_CUDA_TRY(cudaFuncSetAttribute(topk_kernel<LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::kSmem),
+  UMAPB_CUDA_TRY(cudaGetDevice(&dev), "knn_brute: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute: device index %d", dev);
+  if (!attr_set[dev]) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(topk_kernel<LCAP, PAIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        C::kSmem),
                    "knn_brute: set smem attribute");
     attr_set[dev] = true;
   }
-  topk_kernel<LCAP><<<(unsigned)p.grid, THREADS, C::kSmem, stream>>>(
+  return UMAPB_OK;
+}
+
+static int64_t resident_pairs() {
+  static std::mutex mu;
+  static int64_t cached[64];
+  static bool known[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!known[dev]) {
+    int64_t pairs = 0;
+    if (set_smem_attr<32, true>() == UMAPB_OK) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = 2;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(2 * (unsigned)num_sms(), 1, 1);
+      cfg.blockDim = dim3(THREADS, 1, 1);
+      cfg.dynamicSmemBytes = Cfg<32, true>::kSmem;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&clusters, topk_kernel<32, true>, &cfg) == cudaSuccess) pairs = clusters;
+    }
+    cudaGetLastError();  // a refused query only disables pairing
+    clear_error();
+    cached[dev] = pairs;
+    known[dev] = true;
+  }
+  return cached[dev];
+}
+
+template <int LCAP>
+static int launch_topk(const Plan& p, const CUtensorMap& ta, const CUtensorMap& tb, cudaStream_t stream) {
+  int s = set_smem_attr<LCAP, false>();
+  if (s) return s;
+  topk_kernel<LCAP, false><<<(unsigned)p.grid, THREADS, Cfg<LCAP, false>::kSmem, stream>>>(
       ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles, p.slots, p.L, p.cand_s, p.cand_i, p.status);
   UMAPB_LAUNCH_CHECK("knn_brute: topk kernel launch");
   return UMAPB_OK;
+}
+
+static int launch_topk_pair(const Plan& p, const CUtensorMap& ta, const CUtensorMap& tb, cudaStream_t stream) {
+  int s = set_smem_attr<32, true>();
+  if (s) return s;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(2 * (unsigned)p.grid, 1, 1);
+  cfg.blockDim = dim3(THREADS, 1, 1);
+  cfg.dynamicSmemBytes = Cfg<32, true>::kSmem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  UMAPB_CUDA_TRY(cudaLaunchKernelEx(&cfg, topk_kernel<32, true>, ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles,
+                                    p.slots, p.L, p.cand_s, p.cand_i, p.status),
+                 "knn_brute: pair topk kernel launch");
+  return UMAPB_OK;
+}
+
+// Tensor maps of both operands (B box: the CTA's share of a 256-point tile) and
+// the tile kernel the plan chose.
+static int run_tiles(const Plan& p, cudaStream_t stream) {
+  CUtensorMap ta, tb;
+  int s;
+  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)p.n, (uint64_t)p.ld, (uint64_t)p.ld, BM, BK))) return s;
+  if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)p.n, (uint64_t)p.ld, (uint64_t)p.ld, p.pair ? BN / 2 : BN, BK)))
+    return s;
+  if (p.pair) return launch_topk_pair(p, ta, tb, stream);
+  if (p.lcap == 32) return launch_topk<32>(p, ta, tb, stream);
+  if (p.lcap == 64) return launch_topk<64>(p, ta, tb, stream);
+  return launch_topk<128>(p, ta, tb, stream);
 }
 
 static int next_pow2(int v) {
@@ -715,16 +900,7 @@ extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, 
     knn::prep_kernel<<<blocks, 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
     UMAPB_LAUNCH_CHECK("knn_brute: prep kernel launch");
   }
-  CUtensorMap ta, tb;
-  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BM, knn::BK))) return s;
-  if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BN, knn::BK))) return s;
-  if (p.lcap == 32)
-    s = knn::launch_topk<32>(p, ta, tb, stream);
-  else if (p.lcap == 64)
-    s = knn::launch_topk<64>(p, ta, tb, stream);
-  else
-    s = knn::launch_topk<128>(p, ta, tb, stream);
-  if (s) return s;
+  if ((s = knn::run_tiles(p, stream))) return s;
   {
     const int P = knn::next_pow2(p.slots * p.L);
     const int PL = knn::next_pow2(p.L);
@@ -814,16 +990,7 @@ extern "C" int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int
                  "knn_brute_noalloc: candidate reset");
   knn::prep_kernel<<<(unsigned)ceil_div(n * 32, 256), 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
   UMAPB_LAUNCH_CHECK("knn_brute_noalloc: prep kernel launch");
-  CUtensorMap ta, tb;
-  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BM, knn::BK))) return s;
-  if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)n, (uint64_t)p.ld, (uint64_t)p.ld, knn::BN, knn::BK))) return s;
-  if (p.lcap == 32)
-    s = knn::launch_topk<32>(p, ta, tb, stream);
-  else if (p.lcap == 64)
-    s = knn::launch_topk<64>(p, ta, tb, stream);
-  else
-    s = knn::launch_topk<128>(p, ta, tb, stream);
-  if (s) return s;
+  if ((s = knn::run_tiles(p, stream))) return s;
   const int P = knn::next_pow2(p.slots * p.L);
   const int PL = knn::next_pow2(p.L);
   const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);

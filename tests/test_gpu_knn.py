@@ -115,3 +115,43 @@ def test_compute_knn_plug_point(gauss2000, golden):
     idx2, d2 = compute_knn(gauss2000, 15, method="brute", return_euclidean=False)
     np.testing.assert_allclose(np.sqrt(d2), dist, rtol=1e-6)
     assert np.mean(idx == golden("knn_brute_gauss")["idx"]) > 0.999
+
+
+@pytest.fixture(params=["pair", "single"])
+def tile_path(request, monkeypatch):
+    """L <= 32 runs on CTA pairs (256-row tiles, tcgen05 cta_group::2) unless
+    UMAPB_KNN_PAIR=0 selects the one-CTA 128-row tiles; both must be exact."""
+    monkeypatch.setenv("UMAPB_KNN_PAIR", "1" if request.param == "pair" else "0")
+    return request.param
+
+
+@pytest.mark.parametrize("n,d,k", [(2, 3, 1), (129, 65, 15), (255, 40, 15), (256, 64, 15), (257, 130, 15),
+                                   (300, 784, 15), (383, 17, 16), (513, 100, 15), (5000, 32, 15)])
+def test_brute_tile_paths_ragged(n, d, k, tile_path):
+    rng = np.random.default_rng(n * 7 + d)
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    idx, dist = run_knn(X, k)
+    assert_exact_knn(X, idx, dist, k)
+
+
+def test_brute_tile_paths_agree_at_scale(tile_path):
+    """20000 x 784 (several row blocks per unit, candidate slots > 1): sampled
+    rows against the float64 exact kNN."""
+    from mlx_vis_b200 import datasets
+
+    X = datasets.prototype_mixture(20000, 784, seed=0)
+    idx, dist = run_knn(X, 15)
+    rows = np.random.default_rng(1).choice(X.shape[0], 300, replace=False)
+    Xd = X.astype(np.float64)
+    sq = np.sum(Xd * Xd, axis=1)
+    D = sq[rows, None] + sq[None, :] - 2.0 * (Xd[rows] @ Xd.T)
+    D[np.arange(len(rows)), rows] = np.inf
+    cand = np.argpartition(D, 40, axis=1)[:, :40]  # exact top-15 lies among them
+    for i, r in enumerate(rows):
+        c = cand[i]
+        d2 = np.sum((Xd[c] - Xd[r]) ** 2, axis=1)
+        o = np.lexsort((c, d2))[:15]
+        want = d2[o]
+        ours = np.sum((Xd[idx[r]] - Xd[r]) ** 2, axis=1)
+        assert np.all(np.abs(ours - want) <= TIE * np.maximum(want, 1e-12) + 1e-12), r
+        np.testing.assert_allclose(dist[r], np.sqrt(want), rtol=2e-6, atol=1e-6)
