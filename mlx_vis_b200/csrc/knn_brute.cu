@@ -46,8 +46,6 @@ constexpr int UK = 16;   // K of one tcgen05.mma kind::f16
 constexpr int A_BYTES = BM * BK * 2;
 constexpr int THREADS = 256;  // warp 0 TMA, warp 1 MMA, warp 2 TMEM owner, warps 4-7 epilogue
 
-constexpr int BUF = 48;        // per-row hit buffer (entries) of the batched selection
-constexpr int MERGE_AT = 16;   // merge once some row of the warp holds this many hits
 constexpr int STG_PITCH = 36;  // floats per staging row (32 scores + padding)
 
 // LCAP == 32: each thread keeps its row's best 32 (score, column) pairs sorted in
@@ -63,8 +61,12 @@ struct Cfg {
   static constexpr int kBBytes = (PAIR ? BN / 2 : BN) * BK * 2;
   static constexpr int kStageBytes = A_BYTES + kBBytes;
   static constexpr int kRowsPerBlock = PAIR ? 2 * BM : BM;
-  static constexpr int kStages = PAIR ? 4 : (LCAP <= 64 ? 3 : 2);
-  static constexpr int kListBytes = kWarpSelect ? BM * BUF * 8 + BM * STG_PITCH * 4 : BM * LCAP * 8;
+  static constexpr int kStages = PAIR ? 5 : (LCAP <= 64 ? 3 : 2);
+  // batched selection: merge once some row of the warp holds kMergeAt hits; a
+  // 32-column group then adds at most 32 to the kMergeAt - 1 already pending
+  static constexpr int kMergeAt = PAIR ? 12 : 16;
+  static constexpr int kBuf = kMergeAt + 32;
+  static constexpr int kListBytes = kWarpSelect ? BM * kBuf * 8 + BM * STG_PITCH * 4 : BM * LCAP * 8;
   static constexpr int kBarBytes = 256;
   static constexpr int kSmem = 1024 + kStages * kStageBytes + kListBytes + kBarBytes;
 };
@@ -256,7 +258,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint64_t* empty = bars + C::kStages;
   uint64_t* tfull = bars + 2 * C::kStages;
   uint64_t* tempty = tfull + 2;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
+  uint64_t* relay = tempty + 2;  // pair, rank 1: its epilogue's releases, forwarded to rank 0
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(relay + 2);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   if constexpr (PAIR) {
@@ -284,8 +287,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     for (int a = 0; a < 2; ++a) {
       tc::mbar_init(&tfull[a], 1);
-      // pair: one arrival per epilogue warp of both CTAs
-      tc::mbar_init(&tempty[a], PAIR ? 8 : 128);
+      // one arrival per epilogue thread, plus (pair) one forwarded from rank 1
+      tc::mbar_init(&tempty[a], PAIR ? 129 : 128);
+      tc::mbar_init(&relay[a], 128);
     }
     *abort_flag = 0;
     tc::fence_mbar_init();
@@ -418,17 +422,33 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
       }
     }
+  } else if (PAIR && warp == 3) {
+    // ---------------- release relay (pair, rank 1) ----------------
+    // Once rank 1's epilogue has drained an accumulator (128 CTA-scope arrivals
+    // on relay[acc], acquired here), one cluster-scope arrival on rank 0's
+    // tempty[acc] hands it back to the MMA issuer.
+    if (lane == 0 && rank == 1) {
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      for (int64_t t = t_begin; t < t_end; ++t) {
+        if (!tc::mbar_wait(&relay[acc], acc_phase, abort_flag)) break;
+        tc::mbar_arrive_cluster(tc::mapa_shared(tc::smem_u32(&tempty[acc]), 0));
+        acc ^= 1;
+        if (acc == 0) acc_phase ^= 1;
+      }
+    }
   } else if (C::kWarpSelect && warp >= 4) {
     // ---------------- epilogue: batched per-row top-32 (L <= 32) ----------------
     // Thread r of the four epilogue warps owns TMEM lane r, i.e. query row
     // rb*128 + r.  It keeps the row's best 32 (score, column) pairs sorted in
     // registers (lv/li; lv[31] is the admission threshold) and appends every hit
-    // to its own BUF-entry buffer in shared memory (two stores, no loop).  When a
-    // thread of the warp holds MERGE_AT hits the whole warp merges its buffers in
+    // to its own kBuf-entry buffer in shared memory (two stores, no loop).  When a
+    // thread of the warp holds kMergeAt hits the whole warp merges its buffers in
     // batches of 16 with a bitonic sort network and a bitonic 32+16 merge —
     // data-independent, so the 32 rows of a warp run in lockstep.
     const int q = warp & 3;
     const int r = q * 32 + lane;
+    constexpr int BUF = C::kBuf;
     float* bs = list_s;                                          // [BUF][BM]
     int32_t* bi = reinterpret_cast<int32_t*>(list_s + BUF * BM);  // [BUF][BM]
     // per-thread staging row for the chunk being appended; a pitch of 36 floats
@@ -491,7 +511,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     for (int64_t t = t_begin; t < t_end; ++t) {
       const int64_t rb = t / col_tiles;
       const int ct = (int)(t % col_tiles);
-      if (rb != cur_rb) {
+      const bool fresh = rb != cur_rb;  // warp-uniform: the lists are empty
+      if (fresh) {
         if (cur_rb >= 0) flush(cur_rb);
         cur_rb = rb;
       }
@@ -504,6 +525,37 @@ __global__ void __launch_bounds__(THREADS, 1)
       const bool row_ok = row < n;
       const int self_col = row_ok ? (int)row : -1;
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+      // Admission cap of the first tile of a row block, where the empty list
+      // would admit every column: per 32-column group the 4th smallest valid
+      // score, maximised over the groups.  At least 4 x 8 = 32 valid scores are
+      // <= that value, so the row's 32 best of the tile all are, and admitting
+      // scores <= cap alone keeps the list exact while cutting the first tile's
+      // hits from 256 to about the best fifth.  A group with fewer than 4 valid
+      // columns leaves the cap infinite.
+      float cap = INFINITY;
+      if (fresh) {
+        float hi = -INFINITY;
+#pragma unroll 1
+        for (int ch = 0; ch < BN / 32; ++ch) {
+          float v[32];
+          __syncwarp();
+          tc::tmem_ld32(taddr + ch * 32, v);
+          const int col0 = ct * BN + ch * 32;
+          float a0 = INFINITY, a1 = INFINITY, a2 = INFINITY, a3 = INFINITY;  // 4 smallest, sorted
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = col0 + j;
+            const float x = (col != self_col && col < n) ? v[j] : INFINITY;
+            a3 = fminf(a3, fmaxf(a2, x));
+            a2 = fminf(a2, fmaxf(a1, x));
+            a1 = fminf(a1, fmaxf(a0, x));
+            a0 = fminf(a0, x);
+          }
+          hi = fmaxf(hi, a3);
+        }
+        // v <= hi  <=>  v < next float above hi (hi finite); infinite hi admits all
+        cap = hi < INFINITY ? nextafterf(hi, INFINITY) : INFINITY;
+      }
 #pragma unroll 1
       for (int ch = 0; ch < BN / 32; ++ch) {
         float v[32];
@@ -512,7 +564,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int col0 = ct * BN + ch * 32;
         // branch-free hit mask of the 32 columns (four independent OR chains);
         // rows past n never admit
-        const float tau = row_ok ? lv[31] : -INFINITY;
+        const float tau = row_ok ? fminf(lv[31], cap) : -INFINITY;
         unsigned m0 = 0, m1 = 0, m2 = 0, m3 = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -538,16 +590,12 @@ __global__ void __launch_bounds__(THREADS, 1)
             ++cnt;
           }
         }
-        if (__any_sync(0xffffffffu, cnt >= MERGE_AT)) merge_pending();
+        if (__any_sync(0xffffffffu, cnt >= C::kMergeAt)) merge_pending();
       }
       tc::tc_fence_before();
-      if constexpr (PAIR) {
-        // one arrival per warp on rank 0's barrier, which counts both CTAs
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive_cluster(tc::mapa_shared(tc::smem_u32(&tempty[acc]), 0));
-      } else {
-        tc::mbar_arrive(&tempty[acc]);
-      }
+      // CTA-scope arrivals only: a cluster-scope release costs each epilogue
+      // warp over a thousand cycles per tile, so rank 1's warp 3 forwards them
+      tc::mbar_arrive(PAIR && rank == 1 ? &relay[acc] : &tempty[acc]);
       acc ^= 1;
       if (acc == 0) acc_phase ^= 1;
     }
