@@ -110,6 +110,17 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     change flags, *changed (device uint64) += their count,
  *                     *evals (device uint64, nullable) += distances evaluated.
  *                     Rows without a NEW flag are copied on the converging path.
+ *                     Full path only: with nnbuf (from umapb_nnd_join with the same
+ *                     idx_old, mc_new, j_nn) the nn-of-nn distances are read from
+ *                     it, and with curd (and recompute_cur) the current-neighbour
+ *                     distances of positions < mc_new; both nullable.
+ * umapb_nnd_join:     the nn-of-nn candidate distances of one full-path iteration
+ *                     as blocks per source: for every row i and source position
+ *                     p < mc, s = idx_old[i][p], nnbuf[i][p*j_nn + j] =
+ *                     d(i, idx_old[s][j]) for j < j_nn and (curd nullable)
+ *                     curd[i][p] = d(i, s), with the distance rule of
+ *                     umapb_nnd_iteration (FP16 dot rounded when half != 0; FP32
+ *                     rows need dd % 4 == 0).  *evals (nullable) += dots computed.
  * umapb_nnd_sqrt:     Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400).
  * umapb_nnd_random_start: the reference's random start drawn on the device
  *                     (nndescent.py:47-57, 72-82): from the NumPy legacy state in
@@ -131,8 +142,13 @@ int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int32_t dd, int
 int umapb_nnd_reverse_workspace(int64_t n, int32_t k, size_t* bytes);
 int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, void* workspace,
                       size_t workspace_bytes, umapb_stream_t stream);
+int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t* bytes);
+int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
+                   int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf, float* curd,
+                   unsigned long long* evals, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
 int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
-                        const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n, int32_t k,
+                        const float* dist_old, const uint8_t* flags_old, const int32_t* rev, const float* nnbuf,
+                        const float* curd, int64_t n, int32_t k,
                         int32_t mc_new, int32_t j_nn, int32_t converging, int32_t recompute_cur, int32_t* idx_new,
                         float* dist_new, uint8_t* flags_new, unsigned long long* changed,
                         unsigned long long* evals, umapb_stream_t stream);

@@ -27,6 +27,7 @@ control flow, as in the reference.
 
 from __future__ import annotations
 
+import os
 import time
 
 import numpy as np
@@ -167,6 +168,10 @@ class NNDescent:
         changed = torch.zeros(1, dtype=torch.int64, device=dev)
         evals = torch.zeros(1, dtype=torch.int64, device=dev)
         Xh = None
+        # blocked nn-of-nn join (full path); UMAPB_NND_JOIN=0 computes every
+        # candidate distance inside the row kernel instead
+        join_on = os.environ.get("UMAPB_NND_JOIN", "1") != "0"
+        nnbuf = curd = join_ws = None
         self.kernel_log_ = []  # (start event, end event, info) per iteration kernel when profile_kernels
 
         t0 = time.time()
@@ -184,8 +189,8 @@ class NNDescent:
                 # converging path: FP32, full dimension, stored distances
                 ev[0].record() if ev else None
                 call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
-                     ptr(rev if use_rev else None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2),
-                     ptr(changed), ptr(evals), s)
+                     ptr(rev if use_rev else None), ptr(None), ptr(None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2),
+                     ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
                 info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4)
             else:
@@ -214,15 +219,24 @@ class NNDescent:
                         call("umapb_nnd_to_half", ptr(Xd), n, dd, ldx, ptr(src), s)
                 else:
                     src = Xd
+                join = join_on and mc_nn > 0 and (use_half or dd % 4 == 0)
+                if join and nnbuf is None:
+                    nnbuf = torch.empty(n * k * k, dtype=torch.float32, device=dev)
+                    curd = torch.empty((n, k), dtype=torch.float32, device=dev)
+                    join_ws = _lib.workspace(query("umapb_nnd_join_workspace", n, k, k), dev)
                 ev[0].record() if ev else None
+                if join:
+                    call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), n, k, mc_nn, j_nn,
+                         ptr(nnbuf), ptr(curd if recompute else None), ptr(evals), ptr(join_ws), join_ws.numel(), s)
                 call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
-                     ptr(rev if use_rev else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2), ptr(dist2),
-                     ptr(flags2), ptr(changed), ptr(evals), s)
+                     ptr(rev if use_rev else None), ptr(nnbuf if join else None),
+                     ptr(curd if join and recompute else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),
+                     ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
                 if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)
                     call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx2), ptr(dist2), k, 0, s)
                 info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd,
-                            elem=2 if use_half else 4)
+                            elem=2 if use_half else 4, join=join)
             n_changed = int(changed.item())  # the one host read per iteration
             update_frac = n_changed / (n * k)
             idx, idx2 = idx2, idx

@@ -371,6 +371,223 @@ __device__ __forceinline__ void dists_f32(const float* __restrict__ X, int dd, i
   }
 }
 
+
+// ---- blocked join of the nn-of-nn candidates (full-path iterations) ---------------
+// Row i's nn-of-nn candidates are the first j_nn neighbours of each of its first mc
+// neighbours (its sources).  Grouped by source s, they form one dense block: every
+// row i that lists s at a position p < mc, against the columns [s, first j_nn
+// neighbours of s].  One warp per source computes that block; block (i, p) x
+// column 0 is the current-neighbour distance d(i, s) -> curd[i][p], column 1 + j
+// the candidate at the reference's column k + p*j_nn + j -> nnbuf[i][p*j_nn + j].
+// One warp takes one 16-entry chunk of a bucket against all its columns.
+// Each output slot belongs to exactly one (source, entry, column), so the buffers
+// are written without atomics and the result does not depend on the bucket order.
+// A row's vector is read once per source that lists it instead of once per
+// candidate: about mc + 1 + j_nn row reads per row instead of ~k + mc*j_nn + k.
+
+// entries: (i, p) with p < mc, bucketed by s = idx[i][p]; encoded i * 32 + p
+__global__ void src_count_kernel(const int32_t* __restrict__ idx, int64_t n, int k, int mc,
+                                 int32_t* __restrict__ cnt) {
+  const int64_t m = n * mc;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&cnt[idx[(t / mc) * k + (t % mc)]], 1);
+}
+
+__global__ void src_fill_kernel(const int32_t* __restrict__ idx, int64_t n, int k, int mc,
+                                const int32_t* __restrict__ off, int32_t* __restrict__ fill,
+                                int32_t* __restrict__ entries) {
+  const int64_t m = n * mc;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = t / mc;
+    const int p = (int)(t % mc);
+    const int sidx = idx[i * k + p];
+    entries[off[sidx] + atomicAdd(&fill[sidx], 1)] = (int32_t)(i * 32 + p);
+  }
+}
+
+// work items: 16-entry chunks of each bucket (hub sources, listed by hundreds of
+// rows once the graph settles, spread over many warps); nch[s] = chunks of s
+__global__ void chunk_count_kernel(const int32_t* __restrict__ off, int64_t n, int32_t* __restrict__ nch) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+    nch[s] = (off[s + 1] - off[s] + 15) >> 4;
+}
+
+__global__ void chunk_fill_kernel(const int32_t* __restrict__ choff, int64_t n, int32_t* __restrict__ chunk_src) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+    for (int c = choff[s]; c < choff[s + 1]; ++c) chunk_src[c] = (int32_t)s;
+}
+
+struct JoinArgs {
+  const void* Xd;  // float or __half rows of length dd, pitch ldx elements
+  const float* sqd;
+  int dd, ldx;
+  const int32_t* idx_old;
+  const int32_t* off;      // n + 1 bucket offsets
+  const int32_t* entries;  // i * 32 + p, bucketed by source
+  const int32_t* choff;    // n + 1 chunk offsets (choff[n] = chunks)
+  const int32_t* chunk_src;
+  int64_t n;
+  int k, mc, j_nn;
+  int half_round;
+  float* nnbuf;  // (n, mc * j_nn)
+  float* curd;   // (n, k), nullable: current-neighbour distances not wanted
+  unsigned long long* evals;  // nullable
+};
+
+__device__ __forceinline__ int join_col_id(const JoinArgs& a, int64_t s, int col) {
+  return col == 0 ? (int)s : a.idx_old[s * a.k + col - 1];
+}
+
+__device__ __forceinline__ void join_store(const JoinArgs& a, int64_t s, int ent, int col, float dot) {
+  const int64_t i = ent >> 5;
+  const int p = ent & 31;
+  const int cid = join_col_id(a, s, col);
+  const float d = d2_from_dot(a.sqd[i], a.sqd[cid], dot, a.half_round != 0);
+  if (col == 0) {
+    if (a.curd) a.curd[i * a.k + p] = d;
+  } else {
+    a.nnbuf[i * (int64_t)(a.mc * a.j_nn) + p * a.j_nn + (col - 1)] = d;
+  }
+}
+
+// FP16 rows: 16 entries x 16 columns per tile on mma.m16n8k16 (two n-tiles), with
+// the k-position map of dists_f16: thread (g, c) loads 16-byte chunk c + 4 st of
+// entry rows g, g + 8 and of column rows g, g + 8, so A and B share the map and
+// D[m][n] is the full dot product.  D fragments: d0 = columns 2c, 2c + 1 of rows
+// g, g + 8; d1 = columns 8 + 2c, 9 + 2c.
+__global__ void __launch_bounds__(kWarps * 32) join_f16_kernel(JoinArgs a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
+  if (w >= a.choff[a.n]) return;
+  const int64_t s = a.chunk_src[w];
+  const int beg = a.off[s] + 16 * (int)(w - a.choff[s]);
+  const int end = min(a.off[s + 1], beg + 16);
+  const int ncol = 1 + a.j_nn;
+  const __half* X = reinterpret_cast<const __half*>(a.Xd);
+  const int V = a.ldx / 8, S = (V + 3) / 4;
+  const int g = lane >> 2, c = lane & 3;
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+  for (int cb = 0; cb < ncol; cb += 16) {
+    const bool bv0 = cb + g < ncol, bv1 = cb + g + 8 < ncol;
+    const uint4* b0 = reinterpret_cast<const uint4*>(X + (int64_t)(bv0 ? join_col_id(a, s, cb + g) : 0) * a.ldx);
+    const uint4* b1 = reinterpret_cast<const uint4*>(X + (int64_t)(bv1 ? join_col_id(a, s, cb + g + 8) : 0) * a.ldx);
+    for (int e0 = beg; e0 < end; e0 += 16) {
+      const bool av0 = e0 + g < end, av1 = e0 + g + 8 < end;
+      const int en0 = av0 ? a.entries[e0 + g] : 0, en1 = av1 ? a.entries[e0 + g + 8] : 0;
+      const uint4* r0 = reinterpret_cast<const uint4*>(X + (int64_t)(en0 >> 5) * a.ldx);
+      const uint4* r1 = reinterpret_cast<const uint4*>(X + (int64_t)(en1 >> 5) * a.ldx);
+      float d0[4] = {0.f, 0.f, 0.f, 0.f}, d1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+      for (int st = 0; st < S; ++st) {
+        const int q = c + 4 * st;
+        const bool in = q < V;
+        const uint4 A0 = (in && av0) ? __ldg(r0 + q) : zero;
+        const uint4 A1 = (in && av1) ? __ldg(r1 + q) : zero;
+        const uint4 B0 = (in && bv0) ? __ldg(b0 + q) : zero;
+        const uint4 B1 = (in && bv1) ? __ldg(b1 + q) : zero;
+        mma_f16(d0, A0.x, A1.x, A0.y, A1.y, B0.x, B0.y);
+        mma_f16(d0, A0.z, A1.z, A0.w, A1.w, B0.z, B0.w);
+        mma_f16(d1, A0.x, A1.x, A0.y, A1.y, B1.x, B1.y);
+        mma_f16(d1, A0.z, A1.z, A0.w, A1.w, B1.z, B1.w);
+      }
+      // this thread's outputs: rows g (en0), g + 8 (en1) x columns cb + {2c, 2c+1, 8+2c, 9+2c}
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const bool rv = h == 0 ? av0 : av1;
+        const int en = h == 0 ? en0 : en1;
+        if (!rv) continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int col = cb + (u < 2 ? 2 * c + u : 8 + 2 * c + (u - 2));
+          const float dot = u < 2 ? d0[2 * h + u] : d1[2 * h + (u - 2)];
+          if (col < ncol) join_store(a, s, en, col, dot);
+        }
+      }
+    }
+  }
+  if (lane == 0 && a.evals) {
+    const unsigned long long m = (unsigned long long)(end - beg);
+    atomicAdd(a.evals, m * (unsigned long long)ncol);
+  }
+}
+
+// FP32 rows (dd % 4 == 0, 16-byte aligned): 16 entries x 16 columns per tile.  The
+// two half-warps take alternate float4 chunks of the rows; in each, lane m holds
+// entry rows 4(m/4) .. +3 x columns 4(m%4) .. +3 (eight float4 loads feed 64 FMAs),
+// and one shuffle per output adds the halves.
+__global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
+  if (w >= a.choff[a.n]) return;
+  const int64_t s = a.chunk_src[w];
+  const int beg = a.off[s] + 16 * (int)(w - a.choff[s]);
+  const int end = min(a.off[s + 1], beg + 16);
+  const int ncol = 1 + a.j_nn;
+  const float* X = reinterpret_cast<const float*>(a.Xd);
+  const int V = a.dd / 4;
+  const int half = lane >> 4, m = lane & 15;
+  const int ar = (m >> 2) * 4;  // entry rows ar .. ar + 3 of the chunk
+  const int bc = (m & 3) * 4;   // columns bc .. bc + 3 of the block
+  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+  bool av[4];
+  int en[4];
+  const float4* arow[4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    av[u] = beg + ar + u < end;
+    en[u] = av[u] ? a.entries[beg + ar + u] : 0;
+    arow[u] = reinterpret_cast<const float4*>(X + (int64_t)(en[u] >> 5) * a.ldx);
+  }
+  for (int cb = 0; cb < ncol; cb += 16) {
+    const float4* brow[4];
+    bool bv[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      bv[j] = cb + bc + j < ncol;
+      brow[j] = reinterpret_cast<const float4*>(X + (int64_t)(bv[j] ? join_col_id(a, s, cb + bc + j) : 0) * a.ldx);
+    }
+    float acc[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[u][j] = 0.f;
+#pragma unroll 1
+    for (int q = half; q < V; q += 2) {
+      float4 x[4], y[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) x[u] = av[u] ? __ldg(arow[u] + q) : zero;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) y[j] = bv[j] ? __ldg(brow[j] + q) : zero;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[u][j] = fmaf(x[u].x, y[j].x, acc[u][j]);
+          acc[u][j] = fmaf(x[u].y, y[j].y, acc[u][j]);
+          acc[u][j] = fmaf(x[u].z, y[j].z, acc[u][j]);
+          acc[u][j] = fmaf(x[u].w, y[j].w, acc[u][j]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[u][j] += __shfl_xor_sync(0xffffffffu, acc[u][j], 16);
+    if (half == 0) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!av[u]) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (bv[j]) join_store(a, s, en[u], cb + bc + j, acc[u][j]);
+      }
+    }
+  }
+  if (lane == 0 && a.evals) {
+    const unsigned long long mm = (unsigned long long)(end - beg);
+    atomicAdd(a.evals, mm * (unsigned long long)ncol);
+  }
+}
+
 // dedup hash (4 hcap bytes), later candidate distances (4 tcap) + to-do list (2 tcap)
 __host__ __device__ inline size_t iter_scratch_bytes(int tcap, int hcap) {
   const size_t a = (size_t)hcap * 4, b = (size_t)tcap * 6;
@@ -386,6 +603,8 @@ struct IterArgs {
   const float* dist_old;
   const uint8_t* flags_old;  // converging path only
   const int32_t* rev;        // nullable
+  const float* nnbuf;        // nullable: nn-of-nn distances from the blocked join
+  const float* curd;         // nullable: current-neighbour distances from the join
   int64_t n;
   int k, mc_new, j_nn;
   int converging, recompute_cur, half_round;
@@ -496,8 +715,15 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
     float d = kBig;
     bool need = false;
     if ((keep >> ch) & 1ull) {
-      if (t < k && !a.recompute_cur) d = a.dist_old[row * k + t];
-      else need = true;
+      if (t < k) {
+        if (!a.recompute_cur) d = a.dist_old[row * k + t];
+        else if (a.curd && t < a.mc_new) d = a.curd[row * k + t];
+        else need = true;
+      } else if (a.nnbuf && t < k + nn_cols) {
+        d = a.nnbuf[row * nn_cols + (t - k)];
+      } else {
+        need = true;
+      }
     }
     cd[t] = d;
     const unsigned nb = __ballot_sync(0xffffffffu, need);
@@ -677,9 +903,96 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   return UMAPB_OK;
 }
 
+extern "C" int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t* bytes) {
+  clear_error();
+  UMAPB_REQUIRE(bytes && n >= 1 && k >= 1 && mc >= 0 && mc <= k, "nnd_join_workspace: bad arguments");
+  Carver c(nullptr);
+  c.take<int32_t>(64);
+  c.take<int32_t>((size_t)n + 1);                // source counts -> bucket offsets
+  c.take<int32_t>((size_t)n + 1);                // fill counters
+  c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));  // entries
+  c.take<int32_t>((size_t)n + 1);                // chunk counts -> chunk offsets
+  c.take<int32_t>((size_t)n + (size_t)n * mc / 16 + 1);  // chunk -> source
+  c.take<int64_t>(8);
+  *bytes = c.bytes();
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
+                              const int32_t* idx_old, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf,
+                              float* curd, unsigned long long* evals, void* workspace, size_t workspace_bytes,
+                              umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(Xd && sqd && idx_old, "nnd_join: null array argument");
+  UMAPB_REQUIRE(n >= 2 && dd >= 1 && ldx >= dd, "nnd_join: bad shape");
+  UMAPB_REQUIRE(n < ((int64_t)1 << 26), "nnd_join: n must be below 2^26");
+  UMAPB_REQUIRE(k >= 1 && k <= 32, "nnd_join: k must be in [1, 32]");
+  UMAPB_REQUIRE(mc >= 0 && mc <= k && j_nn >= 0 && j_nn <= k, "nnd_join: bad mc / j_nn");
+  UMAPB_REQUIRE(!(mc > 0 && j_nn > 0) || nnbuf, "nnd_join: nnbuf is null");
+  if (half)
+    UMAPB_REQUIRE(ldx % 8 == 0 && (reinterpret_cast<uintptr_t>(Xd) & 15) == 0,
+                  "nnd_join: FP16 rows need a pitch that is a multiple of 8 and a 16-byte aligned base");
+  else
+    UMAPB_REQUIRE(dd % 4 == 0 && ldx % 4 == 0 && (reinterpret_cast<uintptr_t>(Xd) & 15) == 0,
+                  "nnd_join: FP32 rows need dd and the pitch multiples of 4 and a 16-byte aligned base");
+  Carver c(workspace);
+  c.take<int32_t>(64);
+  int32_t* off = c.take<int32_t>((size_t)n + 1);
+  int32_t* fill = c.take<int32_t>((size_t)n + 1);
+  int32_t* entries = c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));
+  int32_t* choff = c.take<int32_t>((size_t)n + 1);
+  const int64_t max_chunks = n + n * mc / 16;  // sum of ceil(count / 16) <= n + n*mc/16
+  int32_t* chunk_src = c.take<int32_t>((size_t)max_chunks + 1);
+  int64_t* total = c.take<int64_t>(8);
+  if (!workspace || workspace_bytes < c.bytes())
+    return set_error(UMAPB_ERR_WORKSPACE, "nnd_join: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
+  if (mc == 0) return UMAPB_OK;
+  const int64_t m = n * mc;
+  UMAPB_CUDA_TRY(cudaMemsetAsync(off, 0, sizeof(int32_t) * (n + 1), stream), "nnd_join: reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(fill, 0, sizeof(int32_t) * (n + 1), stream), "nnd_join: reset");
+  const int64_t want = ceil_div(m, 256);
+  const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
+  nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off);
+  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n + 1, total);
+  nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off, fill, entries);
+  const unsigned sblocks = (unsigned)ceil_div(n, 256);
+  UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
+  nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, n, choff);
+  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(choff, n + 1, total);
+  nnd::chunk_fill_kernel<<<sblocks, 256, 0, stream>>>(choff, n, chunk_src);
+  nnd::JoinArgs a;
+  a.Xd = Xd;
+  a.sqd = sqd;
+  a.dd = dd;
+  a.ldx = ldx;
+  a.idx_old = idx_old;
+  a.off = off;
+  a.entries = entries;
+  a.choff = choff;
+  a.chunk_src = chunk_src;
+  a.n = n;
+  a.k = k;
+  a.mc = mc;
+  a.j_nn = j_nn;
+  a.half_round = half;
+  a.nnbuf = nnbuf;
+  a.curd = curd;
+  a.evals = evals;
+  const unsigned jb = (unsigned)ceil_div(max_chunks, nnd::kWarps);  // warps past the chunk count exit
+  if (half)
+    nnd::join_f16_kernel<<<jb, nnd::kWarps * 32, 0, stream>>>(a);
+  else
+    nnd::join_f32_kernel<<<jb, nnd::kWarps * 32, 0, stream>>>(a);
+  UMAPB_LAUNCH_CHECK("nnd_join kernels");
+  count_launches(7);
+  return UMAPB_OK;
+}
+
 extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
                                    const int32_t* idx_old,
-                                   const float* dist_old, const uint8_t* flags_old, const int32_t* rev, int64_t n,
+                                   const float* dist_old, const uint8_t* flags_old, const int32_t* rev,
+                                   const float* nnbuf, const float* curd, int64_t n,
                                    int32_t k, int32_t mc_new, int32_t j_nn, int32_t converging,
                                    int32_t recompute_cur, int32_t* idx_new, float* dist_new, uint8_t* flags_new,
                                    unsigned long long* changed, unsigned long long* evals,
@@ -709,6 +1022,8 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.dist_old = dist_old;
   a.flags_old = flags_old;
   a.rev = rev;
+  a.nnbuf = converging ? nullptr : nnbuf;
+  a.curd = converging ? nullptr : curd;
   a.n = n;
   a.k = k;
   a.mc_new = mc_new;

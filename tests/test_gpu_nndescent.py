@@ -152,3 +152,79 @@ def test_build_leaves_numpy_stream_like_the_reference():
     random_start(600, 8, 40, 4)
     want = np.random.get_state()
     assert np.array_equal(after[1], want[1]) and after[2:] == want[2:]
+
+
+@pytest.mark.parametrize("half", [False, True])
+@pytest.mark.parametrize("n,d,k,mc,j_nn", [(3000, 64, 15, 15, 15), (1000, 784, 15, 9, 7), (517, 36, 32, 20, 32),
+                                           (40, 8, 5, 3, 2)])
+def test_join_block_distances(n, d, k, mc, j_nn, half):
+    """umapb_nnd_join: nnbuf[i][p*j_nn + j] = d(i, idx[idx[i][p]][j]) and curd[i][p] =
+    d(i, idx[i][p]) with the iteration's distance rule (FP16 dots rounded to FP16)."""
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(n + d + k)
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    idx = rng.integers(0, n - 1, size=(n, k)).astype(np.int32)
+    idx = np.where(idx >= np.arange(n)[:, None], idx + 1, idx).astype(np.int32)
+    Xd = torch.from_numpy(X).cuda()
+    sq = torch.empty(n, dtype=torch.float32, device="cuda")
+    s = _lib.stream_handle()
+    _lib.call("umapb_nnd_sqnorms", _lib.ptr(Xd), n, d, 0, _lib.ptr(sq), s)
+    if half:
+        ldx = (d + 7) // 8 * 8
+        src = torch.zeros((n, ldx), dtype=torch.float16, device="cuda")
+        _lib.call("umapb_nnd_to_half", _lib.ptr(Xd), n, d, ldx, _lib.ptr(src), s)
+        Xv = src[:, :d].float().cpu().numpy().astype(np.float64)
+    else:
+        ldx, src, Xv = d, Xd, X.astype(np.float64)
+    d_idx = torch.from_numpy(idx).cuda()
+    nnbuf = torch.full((n, mc * j_nn), -1.0, dtype=torch.float32, device="cuda")
+    curd = torch.full((n, k), -1.0, dtype=torch.float32, device="cuda")
+    evals = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ws = _lib.workspace(_lib.query("umapb_nnd_join_workspace", n, k, mc), Xd.device)
+    _lib.call("umapb_nnd_join", _lib.ptr(src), _lib.ptr(sq), d, ldx, int(half), _lib.ptr(d_idx), n, k, mc, j_nn,
+              _lib.ptr(nnbuf), _lib.ptr(curd), _lib.ptr(evals), _lib.ptr(ws), ws.numel(), s)
+    got_nn, got_cur = nnbuf.cpu().numpy(), curd.cpu().numpy()
+    assert int(evals.item()) == n * mc * (1 + j_nn)
+    sqh = sq.cpu().numpy().astype(np.float64)
+
+    def want(i, c):
+        dot = np.sum(Xv[i] * Xv[c], axis=-1)
+        if half:
+            dot = dot.astype(np.float32).astype(np.float16).astype(np.float64)
+        return np.maximum(sqh[i] + sqh[c] - 2.0 * dot, 0.0), dot
+
+    rows = np.repeat(np.arange(n), mc)
+    srcs = idx[:, :mc].reshape(-1)
+    w, dot = want(rows, srcs)
+    # FP32 dot sums differ in order; FP16 rounding may then move one FP16 ulp
+    tol = 1e-4 * (sqh[rows] + sqh[srcs]) + (2.5 * np.abs(dot) * 2.0 ** -10 if half else 0.0) + 1e-4
+    assert np.all(np.abs(got_cur[:, :mc].reshape(-1) - w) <= tol)
+    assert np.all(got_cur[:, mc:] == -1.0)  # positions >= mc are not written
+    if j_nn:
+        rr = np.repeat(rows, j_nn)
+        cc = idx[np.repeat(srcs, j_nn), np.tile(np.arange(j_nn), len(srcs))]
+        w2, dot2 = want(rr, cc)
+        tol2 = 1e-4 * (sqh[rr] + sqh[cc]) + (2.5 * np.abs(dot2) * 2.0 ** -10 if half else 0.0) + 1e-4
+        assert np.all(np.abs(got_nn.reshape(-1) - w2) <= tol2)
+
+
+@pytest.mark.parametrize("name,gen", [("gauss", ("gaussian_mixture", 3000, 32, 2)),
+                                      ("proto", ("prototype_mixture", 2000, 784, 3))])
+def test_join_and_row_kernel_builds_agree(name, gen, monkeypatch):
+    """The blocked join changes where the nn-of-nn distances are computed, not the
+    candidates or the rule: the graphs of both builds agree up to FP32 summation order."""
+    from mlx_vis_b200 import NNDescent, datasets
+
+    X = getattr(datasets, gen[0])(gen[1], gen[2], seed=gen[3])
+    out = {}
+    for on in ("1", "0"):
+        monkeypatch.setenv("UMAPB_NND_JOIN", on)
+        nn = NNDescent(k=15, random_state=42)
+        idx, dist = nn.build(X)
+        out[on] = (idx, dist, [h["changed"] for h in nn.history_], [h.get("join") for h in nn.history_])
+    assert any(out["1"][3]) and not any(out["0"][3])
+    assert recall(out["1"][0], out["0"][0]) > 0.995
+    np.testing.assert_allclose(out["1"][2], out["0"][2], rtol=0.02, atol=20)
+    same = out["1"][0] == out["0"][0]
+    np.testing.assert_allclose(out["1"][1][same], out["0"][1][same], rtol=1e-3, atol=1e-3)
