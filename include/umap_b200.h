@@ -113,7 +113,9 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     Full path only: with nnbuf (from umapb_nnd_join with the same
  *                     idx_old, mc_new, j_nn) the nn-of-nn distances are read from
  *                     it, and with curd (and recompute_cur) the current-neighbour
- *                     distances of positions < mc_new; both nullable.
+ *                     distances of positions < mc_new; both nullable.  order
+ *                     (nullable, a permutation of the rows) sets which rows run
+ *                     side by side, for cache locality only.
  * umapb_nnd_join:     the nn-of-nn candidate distances of one full-path iteration
  *                     as blocks per source: for every row i and source position
  *                     p < mc, s = idx_old[i][p], nnbuf[i][p*j_nn + j] =
@@ -121,6 +123,8 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     curd[i][p] = d(i, s), with the distance rule of
  *                     umapb_nnd_iteration (FP16 dot rounded when half != 0; FP32
  *                     rows need dd % 4 == 0).  *evals (nullable) += dots computed.
+ *                     Sources are taken in the order of `order` (nullable, a
+ *                     permutation; for cache locality only).
  * umapb_nnd_sqrt:     Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400).
  * umapb_nnd_random_start: the reference's random start drawn on the device
  *                     (nndescent.py:47-57, 72-82): from the NumPy legacy state in
@@ -144,11 +148,11 @@ int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, vo
                       size_t workspace_bytes, umapb_stream_t stream);
 int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t* bytes);
 int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
-                   int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf, float* curd,
+                   const int32_t* order, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf, float* curd,
                    unsigned long long* evals, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
 int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
-                        const float* dist_old, const uint8_t* flags_old, const int32_t* rev, const float* nnbuf,
-                        const float* curd, int64_t n, int32_t k,
+                        const float* dist_old, const uint8_t* flags_old, const int32_t* rev, const int32_t* order,
+                        const float* nnbuf, const float* curd, int64_t n, int32_t k,
                         int32_t mc_new, int32_t j_nn, int32_t converging, int32_t recompute_cur, int32_t* idx_new,
                         float* dist_new, uint8_t* flags_new, unsigned long long* changed,
                         unsigned long long* evals, umapb_stream_t stream);

@@ -159,6 +159,10 @@ class NNDescent:
             X_low, sq_low = X, sq
         P2_d = P2
 
+        # locality order of the rows (sorted by one random-projection coordinate):
+        # rows and sources that run side by side then share most of their
+        # candidate rows in the L2 cache; it changes no result
+        order = torch.argsort(X_low[:, 0]).to(torch.int32) if n > 1 else None
         rev = torch.empty((n, k), dtype=torch.int32, device=dev)
         rev_ws = _lib.workspace(query("umapb_nnd_reverse_workspace", n, k), dev)
         idx2 = torch.empty_like(idx)
@@ -189,8 +193,8 @@ class NNDescent:
                 # converging path: FP32, full dimension, stored distances
                 ev[0].record() if ev else None
                 call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
-                     ptr(rev if use_rev else None), ptr(None), ptr(None), n, k, mc_conv, j_nn, 1, 0, ptr(idx2),
-                     ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
+                     ptr(rev if use_rev else None), ptr(order), ptr(None), ptr(None), n, k, mc_conv, j_nn, 1, 0,
+                     ptr(idx2), ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
                 info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4)
             else:
@@ -226,10 +230,11 @@ class NNDescent:
                     join_ws = _lib.workspace(query("umapb_nnd_join_workspace", n, k, k), dev)
                 ev[0].record() if ev else None
                 if join:
-                    call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), n, k, mc_nn, j_nn,
-                         ptr(nnbuf), ptr(curd if recompute else None), ptr(evals), ptr(join_ws), join_ws.numel(), s)
+                    call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(order), n, k,
+                         mc_nn, j_nn, ptr(nnbuf), ptr(curd if recompute else None), ptr(evals), ptr(join_ws),
+                         join_ws.numel(), s)
                 call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
-                     ptr(rev if use_rev else None), ptr(nnbuf if join else None),
+                     ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None),
                      ptr(curd if join and recompute else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),
                      ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None

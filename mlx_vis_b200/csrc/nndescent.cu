@@ -407,14 +407,21 @@ __global__ void src_fill_kernel(const int32_t* __restrict__ idx, int64_t n, int 
 
 // work items: 16-entry chunks of each bucket (hub sources, listed by hundreds of
 // rows once the graph settles, spread over many warps); nch[s] = chunks of s
-__global__ void chunk_count_kernel(const int32_t* __restrict__ off, int64_t n, int32_t* __restrict__ nch) {
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-    nch[s] = (off[s + 1] - off[s] + 15) >> 4;
+// Chunks are numbered in the order of `order` (nullable: source ids): position r
+// holds source order[r]; nch[r] = chunks of that source.  An order that puts
+// nearby points next to each other keeps the rows of the chunks in flight within
+// the L2 cache; it changes no result.
+__global__ void chunk_count_kernel(const int32_t* __restrict__ off, const int32_t* __restrict__ order, int64_t n,
+                                   int32_t* __restrict__ nch) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = order ? order[r] : r;
+    nch[r] = (off[s + 1] - off[s] + 15) >> 4;
+  }
 }
 
-__global__ void chunk_fill_kernel(const int32_t* __restrict__ choff, int64_t n, int32_t* __restrict__ chunk_src) {
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
-    for (int c = choff[s]; c < choff[s + 1]; ++c) chunk_src[c] = (int32_t)s;
+__global__ void chunk_fill_kernel(const int32_t* __restrict__ choff, int64_t n, int32_t* __restrict__ chunk_pos) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    for (int c = choff[r]; c < choff[r + 1]; ++c) chunk_pos[c] = (int32_t)r;
 }
 
 struct JoinArgs {
@@ -424,8 +431,9 @@ struct JoinArgs {
   const int32_t* idx_old;
   const int32_t* off;      // n + 1 bucket offsets
   const int32_t* entries;  // i * 32 + p, bucketed by source
-  const int32_t* choff;    // n + 1 chunk offsets (choff[n] = chunks)
-  const int32_t* chunk_src;
+  const int32_t* order;    // nullable: source of position r
+  const int32_t* choff;    // n + 1 chunk offsets by position (choff[n] = chunks)
+  const int32_t* chunk_pos;
   int64_t n;
   int k, mc, j_nn;
   int half_round;
@@ -459,8 +467,9 @@ __global__ void __launch_bounds__(kWarps * 32) join_f16_kernel(JoinArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
   if (w >= a.choff[a.n]) return;
-  const int64_t s = a.chunk_src[w];
-  const int beg = a.off[s] + 16 * (int)(w - a.choff[s]);
+  const int64_t r = a.chunk_pos[w];
+  const int64_t s = a.order ? a.order[r] : r;
+  const int beg = a.off[s] + 16 * (int)(w - a.choff[r]);
   const int end = min(a.off[s + 1], beg + 16);
   const int ncol = 1 + a.j_nn;
   const __half* X = reinterpret_cast<const __half*>(a.Xd);
@@ -519,8 +528,9 @@ __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
   if (w >= a.choff[a.n]) return;
-  const int64_t s = a.chunk_src[w];
-  const int beg = a.off[s] + 16 * (int)(w - a.choff[s]);
+  const int64_t r = a.chunk_pos[w];
+  const int64_t s = a.order ? a.order[r] : r;
+  const int beg = a.off[s] + 16 * (int)(w - a.choff[r]);
   const int end = min(a.off[s + 1], beg + 16);
   const int ncol = 1 + a.j_nn;
   const float* X = reinterpret_cast<const float*>(a.Xd);
@@ -603,6 +613,7 @@ struct IterArgs {
   const float* dist_old;
   const uint8_t* flags_old;  // converging path only
   const int32_t* rev;        // nullable
+  const int32_t* order;      // nullable: row handled by warp slot r (a locality order)
   const float* nnbuf;        // nullable: nn-of-nn distances from the blocked join
   const float* curd;         // nullable: current-neighbour distances from the join
   int64_t n;
@@ -620,7 +631,9 @@ template <class T>
 __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
+  const int64_t slot = (int64_t)blockIdx.x * kWarps + warp;
+  if (slot >= a.n) return;
+  const int64_t row = a.order ? (int64_t)a.order[slot] : slot;
   // per warp: query row | candidate ids | scratch (the dedup hash table, then the
   // candidate distances and the to-do list) | sources
   const size_t xs_bytes = ((size_t)a.ldx * sizeof(T) + 15) / 16 * 16;
@@ -919,7 +932,8 @@ extern "C" int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t
 }
 
 extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
-                              const int32_t* idx_old, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf,
+                              const int32_t* idx_old, const int32_t* order, int64_t n, int32_t k, int32_t mc,
+                              int32_t j_nn, float* nnbuf,
                               float* curd, unsigned long long* evals, void* workspace, size_t workspace_bytes,
                               umapb_stream_t stream_) {
   clear_error();
@@ -943,7 +957,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   int32_t* entries = c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));
   int32_t* choff = c.take<int32_t>((size_t)n + 1);
   const int64_t max_chunks = n + n * mc / 16;  // sum of ceil(count / 16) <= n + n*mc/16
-  int32_t* chunk_src = c.take<int32_t>((size_t)max_chunks + 1);
+  int32_t* chunk_pos = c.take<int32_t>((size_t)max_chunks + 1);
   int64_t* total = c.take<int64_t>(8);
   if (!workspace || workspace_bytes < c.bytes())
     return set_error(UMAPB_ERR_WORKSPACE, "nnd_join: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
@@ -958,9 +972,9 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off, fill, entries);
   const unsigned sblocks = (unsigned)ceil_div(n, 256);
   UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
-  nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, n, choff);
+  nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, order, n, choff);
   scan_exclusive_kernel<<<1, 1024, 0, stream>>>(choff, n + 1, total);
-  nnd::chunk_fill_kernel<<<sblocks, 256, 0, stream>>>(choff, n, chunk_src);
+  nnd::chunk_fill_kernel<<<sblocks, 256, 0, stream>>>(choff, n, chunk_pos);
   nnd::JoinArgs a;
   a.Xd = Xd;
   a.sqd = sqd;
@@ -969,8 +983,9 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   a.idx_old = idx_old;
   a.off = off;
   a.entries = entries;
+  a.order = order;
   a.choff = choff;
-  a.chunk_src = chunk_src;
+  a.chunk_pos = chunk_pos;
   a.n = n;
   a.k = k;
   a.mc = mc;
@@ -992,7 +1007,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
 extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
                                    const int32_t* idx_old,
                                    const float* dist_old, const uint8_t* flags_old, const int32_t* rev,
-                                   const float* nnbuf, const float* curd, int64_t n,
+                                   const int32_t* order, const float* nnbuf, const float* curd, int64_t n,
                                    int32_t k, int32_t mc_new, int32_t j_nn, int32_t converging,
                                    int32_t recompute_cur, int32_t* idx_new, float* dist_new, uint8_t* flags_new,
                                    unsigned long long* changed, unsigned long long* evals,
@@ -1022,6 +1037,7 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.dist_old = dist_old;
   a.flags_old = flags_old;
   a.rev = rev;
+  a.order = order;
   a.nnbuf = converging ? nullptr : nnbuf;
   a.curd = converging ? nullptr : curd;
   a.n = n;

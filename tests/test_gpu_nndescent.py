@@ -182,8 +182,10 @@ def test_join_block_distances(n, d, k, mc, j_nn, half):
     curd = torch.full((n, k), -1.0, dtype=torch.float32, device="cuda")
     evals = torch.zeros(1, dtype=torch.int64, device="cuda")
     ws = _lib.workspace(_lib.query("umapb_nnd_join_workspace", n, k, mc), Xd.device)
-    _lib.call("umapb_nnd_join", _lib.ptr(src), _lib.ptr(sq), d, ldx, int(half), _lib.ptr(d_idx), n, k, mc, j_nn,
-              _lib.ptr(nnbuf), _lib.ptr(curd), _lib.ptr(evals), _lib.ptr(ws), ws.numel(), s)
+    # sources taken in a shuffled order: a scheduling choice that changes no output
+    order = torch.from_numpy(rng.permutation(n).astype(np.int32)).cuda() if n % 2 else None
+    _lib.call("umapb_nnd_join", _lib.ptr(src), _lib.ptr(sq), d, ldx, int(half), _lib.ptr(d_idx), _lib.ptr(order), n,
+              k, mc, j_nn, _lib.ptr(nnbuf), _lib.ptr(curd), _lib.ptr(evals), _lib.ptr(ws), ws.numel(), s)
     got_nn, got_cur = nnbuf.cpu().numpy(), curd.cpu().numpy()
     assert int(evals.item()) == n * mc * (1 + j_nn)
     sqh = sq.cpu().numpy().astype(np.float64)
