@@ -520,11 +520,30 @@ __global__ void __launch_bounds__(kWarps * 32) join_f16_kernel(JoinArgs a) {
   }
 }
 
-// FP32 rows (dd % 4 == 0, 16-byte aligned): 16 entries x 16 columns per tile.  The
-// two half-warps take alternate float4 chunks of the rows; in each, lane m holds
-// entry rows 4(m/4) .. +3 x columns 4(m%4) .. +3 (eight float4 loads feed 64 FMAs),
-// and one shuffle per output adds the halves.
+// FP32 rows (dd % 4 == 0, 16-byte aligned): 16 entries x 16 columns per tile.  Each
+// warp stages its 32 rows (entries 0-15, columns 16-31) slice by slice (32 floats
+// of every row) into its own shared memory with cp.async, JS_STAGES slices in
+// flight, and computes from there: the two half-warps take alternate float4s of a
+// slice, lane m holds entry rows m/4 + {0,4,8,12} x columns m%4 + {0,4,8,12} (eight
+// float4 reads feed 64 FMAs), and one shuffle per output adds the halves.  A row
+// pitch of 40 floats puts the eight 16-byte reads of each instruction on distinct
+// bank groups.
+constexpr int JS_STAGES = 3;
+constexpr int JS_SLICE = 32;  // floats of each row per stage
+constexpr int JS_PITCH = 40;  // floats per staged row
+constexpr int JS_WARP_FLOATS = JS_STAGES * 32 * JS_PITCH;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
+  extern __shared__ __align__(16) float js_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
   if (w >= a.choff[a.n]) return;
@@ -534,50 +553,79 @@ __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
   const int end = min(a.off[s + 1], beg + 16);
   const int ncol = 1 + a.j_nn;
   const float* X = reinterpret_cast<const float*>(a.Xd);
-  const int V = a.dd / 4;
+  const int dd = a.dd;
+  const int nsl = (dd + JS_SLICE - 1) / JS_SLICE;
+  float* buf = js_smem + warp * JS_WARP_FLOATS;
+  const uint32_t buf_s = static_cast<uint32_t>(__cvta_generic_to_shared(buf));
   const int half = lane >> 4, m = lane & 15;
-  const int ar = (m >> 2) * 4;  // entry rows ar .. ar + 3 of the chunk
-  const int bc = (m & 3) * 4;   // columns bc .. bc + 3 of the block
-  const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-  bool av[4];
-  int en[4];
-  const float4* arow[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    av[u] = beg + ar + u < end;
-    en[u] = av[u] ? a.entries[beg + ar + u] : 0;
-    arow[u] = reinterpret_cast<const float4*>(X + (int64_t)(en[u] >> 5) * a.ldx);
-  }
+  const int at = m >> 2;  // entry rows at + 4u
+  const int bt = m & 3;   // columns bt + 4j
+  // this lane copies float4 (lane & 7) of staged rows (lane >> 3) + 4v, v = 0..7
+  const int f4 = lane & 7;
   for (int cb = 0; cb < ncol; cb += 16) {
-    const float4* brow[4];
-    bool bv[4];
+    const float* src[8];
+    bool vrow[8];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      bv[j] = cb + bc + j < ncol;
-      brow[j] = reinterpret_cast<const float4*>(X + (int64_t)(bv[j] ? join_col_id(a, s, cb + bc + j) : 0) * a.ldx);
+    for (int v = 0; v < 8; ++v) {
+      const int sr = (lane >> 3) + 4 * v;
+      int id = 0;
+      if (sr < 16) {
+        vrow[v] = beg + sr < end;
+        if (vrow[v]) id = a.entries[beg + sr] >> 5;
+      } else {
+        vrow[v] = cb + sr - 16 < ncol;
+        if (vrow[v]) id = join_col_id(a, s, cb + sr - 16);
+      }
+      src[v] = X + (int64_t)id * a.ldx + f4 * 4;
     }
+    auto issue = [&](int sl) {
+      if (sl < nsl) {
+        const uint32_t stg = buf_s + (uint32_t)((sl % JS_STAGES) * 32 * JS_PITCH * 4);
+        const int k0 = sl * JS_SLICE + f4 * 4;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int sr = (lane >> 3) + 4 * v;
+          const bool ok = vrow[v] && k0 < dd;  // dd % 4 == 0: a float4 is all in or all out
+          cp_async16(stg + (uint32_t)((sr * JS_PITCH + f4 * 4) * 4), ok ? (const void*)(src[v] + sl * JS_SLICE) : X,
+                     ok ? 16u : 0u);
+        }
+      }
+      cp_async_commit();
+    };
     float acc[4][4];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[u][j] = 0.f;
+#pragma unroll
+    for (int sl = 0; sl < JS_STAGES - 1; ++sl) issue(sl);
 #pragma unroll 1
-    for (int q = half; q < V; q += 2) {
-      float4 x[4], y[4];
+    for (int sl = 0; sl < nsl; ++sl) {
+      cp_async_wait<JS_STAGES - 2>();  // slice sl has landed (this lane's copies)
+      __syncwarp();                   // ... and every lane's; slice sl - 1 is consumed
+      issue(sl + JS_STAGES - 1);       // into the buffer slice sl - 1 used
+      const float* stg = buf + (sl % JS_STAGES) * 32 * JS_PITCH;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) x[u] = av[u] ? __ldg(arow[u] + q) : zero;
+      for (int jj = 0; jj < JS_SLICE / 8; ++jj) {
+        const int c4 = (2 * jj + half) * 4;
+        float4 x[4], y[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) y[j] = bv[j] ? __ldg(brow[j] + q) : zero;
+        for (int u = 0; u < 4; ++u) x[u] = *reinterpret_cast<const float4*>(stg + (at + 4 * u) * JS_PITCH + c4);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+        for (int j = 0; j < 4; ++j) y[j] = *reinterpret_cast<const float4*>(stg + (16 + bt + 4 * j) * JS_PITCH + c4);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          acc[u][j] = fmaf(x[u].x, y[j].x, acc[u][j]);
-          acc[u][j] = fmaf(x[u].y, y[j].y, acc[u][j]);
-          acc[u][j] = fmaf(x[u].z, y[j].z, acc[u][j]);
-          acc[u][j] = fmaf(x[u].w, y[j].w, acc[u][j]);
-        }
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            acc[u][j] = fmaf(x[u].x, y[j].x, acc[u][j]);
+            acc[u][j] = fmaf(x[u].y, y[j].y, acc[u][j]);
+            acc[u][j] = fmaf(x[u].z, y[j].z, acc[u][j]);
+            acc[u][j] = fmaf(x[u].w, y[j].w, acc[u][j]);
+          }
+      }
     }
+    cp_async_wait<0>();
+    __syncwarp();  // the buffers are free for the next column block
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
@@ -585,10 +633,14 @@ __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
     if (half == 0) {
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        if (!av[u]) continue;
+        const int e = beg + at + 4 * u;
+        if (e >= end) continue;
+        const int en = a.entries[e];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (bv[j]) join_store(a, s, en[u], cb + bc + j, acc[u][j]);
+        for (int j = 0; j < 4; ++j) {
+          const int col = cb + bt + 4 * j;
+          if (col < ncol) join_store(a, s, en, col, acc[u][j]);
+        }
       }
     }
   }
@@ -995,10 +1047,19 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   a.curd = curd;
   a.evals = evals;
   const unsigned jb = (unsigned)ceil_div(max_chunks, nnd::kWarps);  // warps past the chunk count exit
-  if (half)
+  if (half) {
     nnd::join_f16_kernel<<<jb, nnd::kWarps * 32, 0, stream>>>(a);
-  else
-    nnd::join_f32_kernel<<<jb, nnd::kWarps * 32, 0, stream>>>(a);
+  } else {
+    const size_t jsmem = (size_t)nnd::kWarps * nnd::JS_WARP_FLOATS * sizeof(float);
+    static bool js_attr = false;
+    if (!js_attr) {
+      UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::join_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)jsmem),
+                     "nnd_join: smem attribute");
+      js_attr = true;
+    }
+    nnd::join_f32_kernel<<<jb, nnd::kWarps * 32, jsmem, stream>>>(a);
+  }
   UMAPB_LAUNCH_CHECK("nnd_join kernels");
   count_launches(7);
   return UMAPB_OK;
