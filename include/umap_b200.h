@@ -112,10 +112,12 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     Rows without a NEW flag are copied on the converging path.
  *                     Full path only: with nnbuf (from umapb_nnd_join with the same
  *                     idx_old, mc_new, j_nn) the nn-of-nn distances are read from
- *                     it, and with curd (and recompute_cur) the current-neighbour
- *                     distances of positions < mc_new; both nullable.  order
- *                     (nullable, a permutation of the rows) sets which rows run
- *                     side by side, for cache locality only.
+ *                     it; with curd (from the same join) the current-neighbour
+ *                     distances of positions < mc_new when recompute_cur, and the
+ *                     distance of a reverse candidate j of row i as curd[j][p] where
+ *                     idx_old[j][p] == i, p < mc_new (the join's d(j, i)); both
+ *                     nullable.  order (nullable, a permutation of the rows) sets
+ *                     which rows run side by side, for cache locality only.
  * umapb_nnd_join:     the nn-of-nn candidate distances of one full-path iteration
  *                     as blocks per source: for every row i and source position
  *                     p < mc, s = idx_old[i][p], nnbuf[i][p*j_nn + j] =

@@ -231,11 +231,10 @@ class NNDescent:
                 ev[0].record() if ev else None
                 if join:
                     call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(order), n, k,
-                         mc_nn, j_nn, ptr(nnbuf), ptr(curd if recompute else None), ptr(evals), ptr(join_ws),
-                         join_ws.numel(), s)
+                         mc_nn, j_nn, ptr(nnbuf), ptr(curd), ptr(evals), ptr(join_ws), join_ws.numel(), s)
                 call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
                      ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None),
-                     ptr(curd if join and recompute else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),
+                     ptr(curd if join else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),
                      ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
                 if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)

@@ -726,7 +726,6 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   } else {
     if (lane < k) srcs[lane] = my_old;
   }
-  for (int t = lane; t < a.ldx; t += 32) xs[t] = reinterpret_cast<const T*>(a.Xd)[row * a.ldx + t];
   for (int t = lane; t < a.hcap; t += 32) htab[t] = -1;
   __syncwarp();
 
@@ -786,6 +785,19 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
         else need = true;
       } else if (a.nnbuf && t < k + nn_cols) {
         d = a.nnbuf[row * nn_cols + (t - k)];
+      } else if (a.curd && t >= k + nn_cols) {
+        // reverse candidate j: this row sits at some position p of j's list, and
+        // for p < mc_new the join computed d(j, row) = d(row, j) as curd[j][p]
+        const int64_t j = cid[t];
+        const int32_t* jr = a.idx_old + j * k;
+        int pos = -1;
+        for (int q = 0; q < a.mc_new; ++q)
+          if (jr[q] == (int)row) {
+            pos = q;
+            break;
+          }
+        if (pos >= 0) d = a.curd[j * k + pos];
+        else need = true;
       } else {
         need = true;
       }
@@ -797,6 +809,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   }
   __syncwarp();
   const float sqi = a.sqd[row];
+  if (n_todo > 0) {  // the query row, for the distances still to compute
+    for (int t = lane; t < a.ldx; t += 32) xs[t] = reinterpret_cast<const T*>(a.Xd)[row * a.ldx + t];
+    __syncwarp();
+  }
   if constexpr (sizeof(T) == 2) {
     dists_f16(reinterpret_cast<const __half*>(a.Xd), a.ldx, reinterpret_cast<const __half*>(xs), a.sqd, sqi, row,
               cid, todo, n_todo, cd, lane);
