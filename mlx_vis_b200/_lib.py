@@ -218,7 +218,9 @@ def legacy_normal(rs, shape, loc: float, scale: float, device, parallel: bool = 
 
 
 def spectral(rows, cols, vals, n_edges, n: int, dim: int, V0: torch.Tensor, noise: torch.Tensor,
-             n_iter: int = 100) -> torch.Tensor:
+             n_iter: int = 100, check: bool = False) -> torch.Tensor:
+    """Spectral initial embedding (n, dim).  ``check`` synchronises and raises if
+    the power iteration's grid barrier gave up."""
     V0 = _require(V0, torch.float32, 2, "V0")
     noise = _require(noise, torch.float32, 2, "noise")
     dev = V0.device
@@ -227,6 +229,8 @@ def spectral(rows, cols, vals, n_edges, n: int, dim: int, V0: torch.Tensor, nois
     Y = torch.empty((n, dim), dtype=torch.float32, device=dev)
     call("umapb_spectral", ptr(rows), ptr(cols), ptr(vals), ptr(n_edges), e_cap, n, dim, ptr(V0), int(n_iter),
          ptr(noise), ptr(Y), ptr(ws), ws.numel(), stream_handle())
+    if check:
+        read_status(ws)
     return Y
 
 

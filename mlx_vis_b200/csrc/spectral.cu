@@ -15,6 +15,7 @@
 // gathered row on the fly and accumulates the new Gram matrix in FP64; its last
 // block factors that Gram matrix for the next iteration.
 #include <math.h>
+#include <stdlib.h>
 
 #include "common.cuh"
 #include "philox.cuh"
@@ -160,6 +161,151 @@ __global__ void spmv_gram_kernel(const float* __restrict__ Vin, const double* __
   }
 }
 
+
+// ---- all power iterations in one cooperative launch ---------------------------
+// The per-iteration launches above spend most of their time starting and ending
+// (100 dependent launches of a few microseconds of work).  Here the grid stays
+// resident: each iteration is the SpMV + Gram step of spmv_gram_kernel over a
+// grid-stride range of rows, then one grid barrier, after which EVERY block
+// factors the completed Gram matrix itself (a few FP64 operations) instead of
+// waiting for a last block.  V rows written by other blocks are read through L2
+// (ld.global.cg).  The barrier gives up after kBarrierLimitNs, raises a shared
+// abort flag and the status word, and every block then returns.
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ bool grid_barrier(unsigned* bar, unsigned target, int* abort_g) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const unsigned long long t0 = gtimer();
+    for (unsigned i = 1;; ++i) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= target) break;
+      if ((i & 255) == 0) {
+        if (*(volatile int*)abort_g) {
+          ok = 0;
+          break;
+        }
+        if (gtimer() - t0 > kBarrierLimitNs) {
+          atomicExch(abort_g, 1);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int KK>  // columns of V: n_components + 1
+__global__ void __launch_bounds__(kBlock) power_kernel(float* __restrict__ V0, float* __restrict__ V1,
+                                                       const int64_t* __restrict__ row_ptr,
+                                                       const int32_t* __restrict__ cols, const float* __restrict__ wn,
+                                                       int64_t n, int n_iter, double* __restrict__ G,
+                                                       double* __restrict__ Rinv, unsigned* __restrict__ bar,
+                                                       int* __restrict__ abort_g, int32_t* __restrict__ status) {
+  constexpr int kk = KK;
+  constexpr int vp = KK <= 4 ? 4 : 8;
+  __shared__ double ri[kMaxCols * kMaxCols];
+  __shared__ double gsum[kBlock / 32][kMaxCols * kMaxCols];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = threadIdx.x & (kLanes - 1);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x / kLanes;  // rows per grid pass
+  if (threadIdx.x < kk * kk) ri[threadIdx.x] = (threadIdx.x % (kk + 1) == 0) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int it = 0; it < n_iter; ++it) {
+    const float* Vin = (it & 1) ? V1 : V0;
+    float* Vout = (it & 1) ? V0 : V1;
+    double* Git = G + (size_t)it * kk * kk;
+    double part[kk * kk];
+#pragma unroll
+    for (int t = 0; t < kk * kk; ++t) part[t] = 0.0;
+    // the loop bound is the warp's first row, so every lane of a warp makes the
+    // same passes and meets the shuffle below; rows past n do no work
+    for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + warp * 32) / kLanes; r0 < n; r0 += stride) {
+      const int64_t r = r0 + lane / kLanes;
+      const bool valid = r < n;
+      double acc[kk];
+#pragma unroll
+      for (int j = 0; j < kk; ++j) acc[j] = 0.0;
+      const int64_t e1 = valid ? row_ptr[r + 1] : 0;
+      for (int64_t e = valid ? row_ptr[r] + sub : 0; e < e1; e += kLanes) {
+        const int64_t c = cols[e];
+        const double w = (double)wn[e];
+        double v[kMaxCols];
+        const float4 a = __ldcg(reinterpret_cast<const float4*>(Vin + c * vp));  // rows padded to 4 or 8
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+        if (kk > 4) v[4] = __ldcg(Vin + c * vp + 4);
+#pragma unroll
+        for (int j = 0; j < kk; ++j) {  // q_j = sum_i v_i Rinv[i][j]
+          double q = 0.0;
+#pragma unroll
+          for (int i = 0; i <= j; ++i) q += v[i] * ri[i * kk + j];
+          acc[j] += w * q;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kk; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 1);  // kLanes == 2
+      if (valid && sub == 0) {
+#pragma unroll
+        for (int j = 0; j < vp; ++j) Vout[r * vp + j] = j < kk ? (float)acc[j] : 0.f;
+#pragma unroll
+        for (int i = 0; i < kk; ++i)
+#pragma unroll
+          for (int j = i; j < kk; ++j) part[i * kk + j] += acc[i] * acc[j];
+      }
+    }
+    // block reduction of the Gram partials, then one atomic per entry and block
+#pragma unroll
+    for (int i = 0; i < kk; ++i) {
+#pragma unroll
+      for (int j = i; j < kk; ++j) {
+        double g = part[i * kk + j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+        if (lane == 0) gsum[warp][i * kk + j] = g;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < kk * kk) {
+      const int i = threadIdx.x / kk, j = threadIdx.x % kk;
+      if (i <= j) {
+        double g = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) g += gsum[w][i * kk + j];
+        atomicAdd(&Git[i * kk + j], g);
+        if (i != j) atomicAdd(&Git[j * kk + i], g);
+      }
+    }
+    if (!grid_barrier(bar, (unsigned)(it + 1) * gridDim.x, abort_g)) {
+      if (threadIdx.x == 0) atomicExch(status, (int32_t)kDevTimeoutEpilogue);
+      return;
+    }
+    if (threadIdx.x == 0) {
+      double Gl[kMaxCols * kMaxCols];
+      for (int t = 0; t < kk * kk; ++t) Gl[t] = __ldcg(Git + t);
+      double rl[kMaxCols * kMaxCols];
+      chol_inverse(Gl, kk, rl);
+      for (int t = 0; t < kk * kk; ++t) ri[t] = rl[t];
+      if (blockIdx.x == 0)
+        for (int t = 0; t < kk * kk; ++t) Rinv[(size_t)it * kk * kk + t] = rl[t];
+    }
+    __syncthreads();
+  }
+}
+
 __device__ __forceinline__ unsigned f2ord(float f) {
   const unsigned u = __float_as_uint(f);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
@@ -225,7 +371,8 @@ struct Layout {
   float* V[2];  // n rows of vp floats (kk values, zero padded to 4 or 8)
   double* G;       // n_iter blocks of kk*kk
   double* Rinv;    // n_iter blocks of kk*kk: the inverse Cholesky factor after each iteration
-  unsigned* done;  // per-iteration block counters
+  unsigned* done;  // per-iteration block counters; done[n_iter] the grid barrier
+  int* abort_g;    // cooperative path: barrier abort flag
   float* emb;
   unsigned* red;  // absmax, colmin[4], colmax[4]
   size_t bytes;
@@ -245,7 +392,8 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   l.V[1] = c.take<float>((size_t)n * vpitch(kk));
   l.G = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
   l.Rinv = c.take<double>((size_t)(n_iter > 0 ? n_iter : 1) * kk * kk);
-  l.done = c.take<unsigned>((size_t)(n_iter > 0 ? n_iter : 1));
+  l.done = c.take<unsigned>((size_t)(n_iter > 0 ? n_iter : 1) + 1);
+  l.abort_g = c.take<int>(1);
   l.emb = c.take<float>((size_t)n * dim);
   l.red = c.take<unsigned>(16);
   l.bytes = c.bytes();
@@ -318,7 +466,8 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   const unsigned rb = (unsigned)ceil_div(n, spectral::kBlock);
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.status, 0, 4, stream), "spectral: status reset");
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.G, 0, sizeof(double) * n_iter * kk * kk, stream), "spectral: gram reset");
-  UMAPB_CUDA_TRY(cudaMemsetAsync(l.done, 0, sizeof(unsigned) * n_iter, stream), "spectral: counter reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.done, 0, sizeof(unsigned) * (n_iter + 1), stream), "spectral: counter reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(l.abort_g, 0, sizeof(int), stream), "spectral: abort reset");
   spectral::row_ptr_kernel<<<(unsigned)ceil_div(n + 1, spectral::kBlock), spectral::kBlock, 0, stream>>>(
       rows, n_edges, n, l.row_ptr);
   spectral::degree_kernel<<<rb, spectral::kBlock, 0, stream>>>(vals, l.row_ptr, n, l.dis);
@@ -330,11 +479,51 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
       V0, n, kk, vp, l.V[0]);
   UMAPB_LAUNCH_CHECK("spectral: setup kernels");
   const unsigned pb = (unsigned)ceil_div(n * spectral::kLanes, spectral::kBlock);
-  for (int it = 0; it < n_iter; ++it) {
-    const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
-    spectral::spmv_gram_kernel<<<pb, spectral::kBlock, 0, stream>>>(
-        l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, vp, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk, l.done + it,
-        l.Rinv + (size_t)it * kk * kk);
+  // one cooperative launch for all iterations (every block resident), sized to
+  // the rows; the per-iteration launches remain for devices that refuse it and
+  // behind UMAPB_SPECTRAL_COOP=0
+  int per_sm = 0;
+  int coop = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+  {
+    const char* e = getenv("UMAPB_SPECTRAL_COOP");
+    if (e && e[0] == '0' && e[1] == 0) coop = 0;
+  }
+  const void* pk = kk == 2   ? (const void*)spectral::power_kernel<2>
+                   : kk == 3 ? (const void*)spectral::power_kernel<3>
+                   : kk == 4 ? (const void*)spectral::power_kernel<4>
+                             : (const void*)spectral::power_kernel<5>;
+  if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, spectral::kBlock, 0) != cudaSuccess)
+    per_sm = 0;
+  cudaGetLastError();
+  int64_t grid = (int64_t)num_sms() * (per_sm < 4 ? per_sm : 4);
+  if (grid > (int64_t)pb) grid = pb;
+  bool launched = false;
+  if (coop && grid > 0) {
+    float* v0 = l.V[0];
+    float* v1 = l.V[1];
+    const int64_t* rp = l.row_ptr;
+    const float* w = l.wn;
+    int64_t nn = n;
+    int ni = n_iter;
+    double* G = l.G;
+    double* R = l.Rinv;
+    unsigned* bar = l.done + n_iter;
+    int* ab = l.abort_g;
+    int32_t* st = l.status;
+    void* args[] = {&v0, &v1, &rp, &cols, &w, &nn, &ni, &G, &R, &bar, &ab, &st};
+    launched = cudaLaunchCooperativeKernel(pk, dim3((unsigned)grid), dim3(spectral::kBlock), args, 0, stream) ==
+               cudaSuccess;
+    if (!launched) cudaGetLastError();
+  }
+  if (!launched) {
+    for (int it = 0; it < n_iter; ++it) {
+      const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
+      spectral::spmv_gram_kernel<<<pb, spectral::kBlock, 0, stream>>>(
+          l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, vp, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk,
+          l.done + it, l.Rinv + (size_t)it * kk * kk);
+    }
   }
   UMAPB_LAUNCH_CHECK("spectral: power iteration");
   spectral::init_red_kernel<<<1, 32, 0, stream>>>(l.red, dim);
@@ -346,7 +535,7 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
                                                                      l.red + 5);
   spectral::minmax_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, n, dim, l.red + 1, l.red + 5, Y);
   UMAPB_LAUNCH_CHECK("spectral: rescale kernels");
-  count_launches((e_cap > 0 ? 3 : 2) + 1 + n_iter + 4);
+  count_launches((e_cap > 0 ? 3 : 2) + 1 + (launched ? 1 : n_iter) + 4);
   return UMAPB_OK;
 }
 

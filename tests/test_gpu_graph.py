@@ -60,7 +60,15 @@ def test_fuzzy_fp32_mode_matches_reference(name, n_epochs, golden):
     assert np.mean(rel <= 1e-5) > 0.99 and rel.max() < 5e-5
 
 
-def test_spectral_matches_reference_with_injected_draws(golden):
+@pytest.fixture(params=["coop", "launches"])
+def spectral_path(request, monkeypatch):
+    """The power iteration runs as one cooperative launch unless UMAPB_SPECTRAL_COOP=0
+    selects one launch per iteration; both must agree with the reference."""
+    monkeypatch.setenv("UMAPB_SPECTRAL_COOP", "1" if request.param == "coop" else "0")
+    return request.param
+
+
+def test_spectral_matches_reference_with_injected_draws(golden, spectral_path):
     from mlx_vis_b200 import _lib
 
     fz, sp = golden("fuzzy_gauss"), golden("spectral_gauss")
@@ -68,10 +76,32 @@ def test_spectral_matches_reference_with_injected_draws(golden):
     rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
     ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
     noise = np.random.RandomState(42).normal(scale=0.0001, size=(n, 2)).astype(np.float32)
-    Y = _lib.spectral(rows, cols, vals, ne, n, 2, cuda(sp["V0"]), cuda(noise), n_iter=100).cpu().numpy()
+    Y = _lib.spectral(rows, cols, vals, ne, n, 2, cuda(sp["V0"]), cuda(noise), n_iter=100,
+                      check=True).cpu().numpy()
     Y64 = ospec.spectral_init(fz["rows"], fz["cols"], fz["vals"], n, sp["V0"], 0, dtype=np.float64)
     assert np.abs(Y - Y64).max() < 1e-4
     assert np.abs(Y - sp["Y0"]).max() < 1e-3
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3, 4])
+def test_spectral_paths_agree_for_every_dim(golden, monkeypatch, dim):
+    """Cooperative and per-iteration power iterations: same sums in FP64, the same
+    embedding up to the order of the Gram matrix's atomic additions."""
+    from mlx_vis_b200 import _lib
+
+    fz = golden("fuzzy_gauss")
+    n = 2000
+    rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
+    ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
+    V0 = np.random.RandomState(dim).normal(size=(n, dim + 1)).astype(np.float32)
+    noise = np.random.RandomState(42).normal(scale=0.0001, size=(n, dim)).astype(np.float32)
+    out = {}
+    for path in ("1", "0"):
+        monkeypatch.setenv("UMAPB_SPECTRAL_COOP", path)
+        out[path] = _lib.spectral(rows, cols, vals, ne, n, dim, cuda(V0), cuda(noise), n_iter=100,
+                                  check=True).cpu().numpy()
+    assert out["1"].shape == (n, dim) and np.all(np.isfinite(out["1"]))
+    assert np.abs(out["1"] - out["0"]).max() < 1e-3
 
 
 def _layout(fz, n=2000, n_epochs=200):
