@@ -790,12 +790,14 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
         // for p < mc_new the join computed d(j, row) = d(row, j) as curd[j][p]
         const int64_t j = cid[t];
         const int32_t* jr = a.idx_old + j * k;
+        // predicated sweeps of 16 positions (no early exit inside a sweep) keep
+        // their loads in flight together; the lowest matching position wins
         int pos = -1;
-        for (int q = 0; q < a.mc_new; ++q)
-          if (jr[q] == (int)row) {
-            pos = q;
-            break;
-          }
+        for (int q0 = 0; q0 < a.mc_new && pos < 0; q0 += 16) {
+#pragma unroll
+          for (int u = 15; u >= 0; --u)
+            if (q0 + u < a.mc_new && __ldg(jr + q0 + u) == (int)row) pos = q0 + u;
+        }
         if (pos >= 0) d = a.curd[j * k + pos];
         else need = true;
       } else {
