@@ -31,5 +31,37 @@ def to_device_f32(X, dev: torch.device | None = None) -> torch.Tensor:
     return host.to(dev, non_blocking=True)
 
 
+def upload_async(X, dev: torch.device | None = None):
+    """Like to_device_f32, but a host array is copied on a side stream: returns
+    (tensor, event), and work that does not read the tensor may run on the current
+    stream meanwhile; make the current stream wait on the event (None when X was
+    already on the device) before the first kernel that reads it."""
+    dev = dev or device()
+    if isinstance(X, torch.Tensor) and X.is_cuda:
+        return to_device_f32(X, dev), None
+    if isinstance(X, torch.Tensor):
+        host = X.detach()
+        if host.dtype != torch.float32:
+            host = host.float()
+        host = host.contiguous()
+    else:
+        a = np.ascontiguousarray(np.asarray(X, dtype=np.float32))
+        host = torch.from_numpy(a)
+    if host.ndim != 2:
+        raise ValueError(f"expected a 2-D array (n_samples, n_features), got shape {tuple(host.shape)}")
+    if not host.is_pinned() and host.numel() * 4 >= (1 << 20):
+        host = host.pin_memory()
+    main = torch.cuda.current_stream(dev)
+    Xd = torch.empty(host.shape, dtype=torch.float32, device=dev)
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(main)  # Xd's allocation is ordered on the current stream
+    with torch.cuda.stream(side):
+        Xd.copy_(host, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(side)
+    Xd.record_stream(side)
+    return Xd, done
+
+
 def to_host(t: torch.Tensor) -> np.ndarray:
     return t.detach().cpu().numpy()

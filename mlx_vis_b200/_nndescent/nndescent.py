@@ -128,11 +128,16 @@ class NNDescent:
         return self.neighbor_graph
 
     # ------------------------------------------------------------------
-    def build_device(self, X: torch.Tensor):
-        """Device version of build: (idx int32, Euclidean dist float32) CUDA tensors."""
+    def build_device(self, X: torch.Tensor, x_ready=None):
+        """Device version of build: (idx int32, Euclidean dist float32) CUDA tensors.
+
+        ``x_ready``: an event that X's upload records (see _device.upload_async);
+        the random start, which does not read X, runs before the wait on it."""
         if not isinstance(X, torch.Tensor) or not X.is_cuda:
             X = to_device_f32(X)
-        X = X.contiguous().float()
+            x_ready = None
+        if x_ready is None:
+            X = X.contiguous().float()
         n, d = X.shape
         if n < 2:
             raise ValueError("NNDescent needs at least 2 points")
@@ -145,6 +150,9 @@ class NNDescent:
         s = stream_handle()
 
         idx, P, P2, rng_state = random_start_device(n, k, d, self.random_state, dev)
+        if x_ready is not None:
+            torch.cuda.current_stream(dev).wait_event(x_ready)
+            X = X.contiguous().float()
         dist = torch.empty((n, k), dtype=torch.float32, device=dev)
         sq = torch.empty(n, dtype=torch.float32, device=dev)
         call("umapb_nnd_sqnorms", ptr(X), n, d, 0, ptr(sq), s)

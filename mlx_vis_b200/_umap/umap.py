@@ -35,7 +35,7 @@ import torch
 
 from mlx_vis_b200 import _lib
 from mlx_vis_b200._curve import find_ab_params
-from mlx_vis_b200._device import device, to_device_f32, to_host
+from mlx_vis_b200._device import device, to_host, upload_async
 from mlx_vis_b200._normalize import normalize_input
 
 
@@ -104,13 +104,18 @@ class UMAP:
         if self.normalize:
             Xh = X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else np.asarray(X, dtype=np.float32)
             X = normalize_input(np.asarray(Xh, dtype=np.float32), self.normalize).astype(np.float32)
-        Xd = to_device_f32(X, dev)
+        # a host X is copied on a side stream; the draws below and NNDescent's
+        # random start do not read X and run while the copy is in flight
+        Xd, x_ready = upload_async(X, dev)
         n, dim = Xd.shape
         if n < 2:
             raise ValueError("UMAP needs at least 2 samples")
+        seed = self.random_state if self.random_state is not None else _random_seed()
+        draws = self._spectral_draws(n, seed, dev) if self.init == "spectral" else None
         ev.mark("upload")
 
         if self.pca_dim is not None and dim > self.pca_dim:
+            x_ready = self._wait(x_ready, dev)
             Xd = self._pca(Xd)
             ev.mark("pca")
 
@@ -124,9 +129,10 @@ class UMAP:
             nn = NNDescent(k=k, verbose=self.verbose,
                            random_state=self.random_state if self.random_state is not None else 42)
             nn.profile_kernels = self.profile_kernels
-            knn_idx, knn_dist = nn.build_device(Xd)
+            knn_idx, knn_dist = nn.build_device(Xd, x_ready=x_ready)
             self.nndescent_ = nn
         else:
+            x_ready = self._wait(x_ready, dev)
             knn_idx, knn_dist = _lib.knn_brute(Xd, k, extra=RERANK_EXTRA)
             self.nndescent_ = None
         ev.mark("knn")
@@ -140,11 +146,10 @@ class UMAP:
 
         a, b = find_ab_params(self.spread, self.min_dist)
         self.a_, self.b_ = a, b
-        seed = self.random_state if self.random_state is not None else _random_seed()
 
         if self.verbose:
             print("Initializing embedding...")
-        Y = self._init_embedding(Xd, rows, cols, vals, n_edges, n, seed)
+        Y = self._init_embedding(Xd, rows, cols, vals, n_edges, n, seed, draws)
         ev.mark("init")
 
         self._optimize(rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback)
@@ -167,7 +172,23 @@ class UMAP:
             print(f"Variance retained: {ret * 100:.1f}%")
         return (Xc @ proj).contiguous()
 
-    def _init_embedding(self, Xd, rows, cols, vals, n_edges, n, seed) -> torch.Tensor:
+    @staticmethod
+    def _wait(x_ready, dev):
+        if x_ready is not None:
+            torch.cuda.current_stream(dev).wait_event(x_ready)
+        return None
+
+    def _spectral_draws(self, n, seed, dev):
+        """The spectral init's random inputs, which depend only on n and the seeds:
+        V0 (n, c + 1) and the reference's noise RandomState(random_state or
+        42).normal(scale=1e-4, size=(n, c)) as float32 (umap.py:344-346), drawn on
+        the device from that stream's state."""
+        c = self.n_components
+        V0 = _lib.normal((n, c + 1), seed, dev)
+        noise_d = _lib.legacy_normal(np.random.RandomState(self.random_state or 42), (n, c), 0.0, 0.0001, dev)
+        return V0, noise_d
+
+    def _init_embedding(self, Xd, rows, cols, vals, n_edges, n, seed, draws=None) -> torch.Tensor:
         c = self.n_components
         dev = Xd.device
         if self.init == "learned":
@@ -179,10 +200,7 @@ class UMAP:
         if self.init != "spectral":
             raise ValueError(f"unknown init {self.init!r}")
         try:
-            V0 = _lib.normal((n, c + 1), seed, dev)
-            # RandomState(random_state or 42).normal(scale=1e-4, size=(n, c)) as float32
-            # (umap.py:344-346), drawn on the device from that stream's state
-            noise_d = _lib.legacy_normal(np.random.RandomState(self.random_state or 42), (n, c), 0.0, 0.0001, dev)
+            V0, noise_d = draws if draws is not None else self._spectral_draws(n, seed, dev)
             Y = _lib.spectral(rows, cols, vals, n_edges, n, c, V0, noise_d, n_iter=100)
             if self.verbose:
                 print("Using spectral initialization")

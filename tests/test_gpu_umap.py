@@ -61,3 +61,33 @@ def test_other_output_dims(n_components):
     X = gaussian_mixture(600, 16, seed=2)
     Y = UMAP(n_components=n_components, n_epochs=60, knn_method="brute", random_state=0).fit_transform(X)
     assert Y.shape == (600, n_components) and np.isfinite(Y).all()
+
+
+@pytest.mark.parametrize("method", ["nndescent", "brute"])
+def test_host_and_device_inputs_give_the_same_fit(gauss2000, method):
+    """A host X (NumPy or pinned torch) is uploaded on a side stream while the
+    random start and the spectral draws run; the fit matches one from an X already
+    on the device up to the layout's float-atomic rounding."""
+    import torch
+
+    from mlx_vis_b200 import UMAP
+
+    tw = []
+    for X in (gauss2000, torch.from_numpy(gauss2000).cuda(), torch.from_numpy(gauss2000).pin_memory()):
+        Y = UMAP(n_epochs=50, knn_method=method, random_state=5).fit_transform(X)
+        assert Y.shape == (2000, 2) and np.isfinite(Y).all()
+        tw.append(trustworthiness(gauss2000, Y, n_neighbors=15))
+    assert max(tw) - min(tw) < 0.003, tw
+
+
+def test_nndescent_waits_for_the_upload_after_its_random_start(gauss2000):
+    import torch
+
+    from mlx_vis_b200 import NNDescent
+    from mlx_vis_b200._device import upload_async
+
+    Xd, ready = upload_async(gauss2000)
+    assert ready is not None
+    idx_a, dist_a = NNDescent(k=15, random_state=7).build_device(Xd, x_ready=ready)
+    idx_b, dist_b = NNDescent(k=15, random_state=7).build_device(torch.from_numpy(gauss2000).cuda())
+    assert torch.equal(idx_a, idx_b) and torch.equal(dist_a, dist_b)
