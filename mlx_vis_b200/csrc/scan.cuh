@@ -6,13 +6,15 @@
 namespace umapb {
 
 // Exclusive scan of `count` int32 values in place by ONE block of 1024 threads;
-// writes the grand total to *total.  Each pass covers 1024 x 8 values: a thread
-// scans its 8 consecutive values in registers (two 16-byte loads), the block scans
-// the thread sums (warp shuffles, then one warp over the 32 warp sums) and a
-// running carry links the passes.
+// writes the grand total to *total.  Each pass covers 1024 x 16 values (one pass
+// for up to 16 K values, five for 70 K): a thread scans its 16 consecutive values
+// in registers (four 16-byte loads), the block scans the thread sums (warp
+// shuffles, then one warp over the 32 warp sums) and a running carry links the
+// passes.
 template <int kDummy = 0>
-__global__ void scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count, int64_t* __restrict__ total) {
-  constexpr int kItems = 8;
+__global__ void __launch_bounds__(1024) scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
+                                                              int64_t* __restrict__ total) {
+  constexpr int kItems = 16;
   __shared__ int64_t warp_sums[32];
   __shared__ int64_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -25,9 +27,11 @@ __global__ void scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
     int32_t v[kItems];
     const bool full = aligned && first + kItems <= count;
     if (full) {
-      const int4 a = *reinterpret_cast<const int4*>(vals + first);
-      const int4 b = *reinterpret_cast<const int4*>(vals + first + 4);
-      v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+#pragma unroll
+      for (int q = 0; q < kItems / 4; ++q) {
+        const int4 a = *reinterpret_cast<const int4*>(vals + first + 4 * q);
+        v[4 * q] = a.x, v[4 * q + 1] = a.y, v[4 * q + 2] = a.z, v[4 * q + 3] = a.w;
+      }
     } else {
 #pragma unroll
       for (int u = 0; u < kItems; ++u) v[u] = first + u < count ? vals[first + u] : 0;
@@ -54,19 +58,20 @@ __global__ void scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
     }
     __syncthreads();
     int64_t run = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
-    int32_t o[kItems];
 #pragma unroll
-    for (int u = 0; u < kItems; ++u) {
-      o[u] = (int32_t)run;
-      run += v[u];
+    for (int u = 0; u < kItems; ++u) {  // exclusive prefix, in place
+      const int32_t t = v[u];
+      v[u] = (int32_t)run;
+      run += t;
     }
     if (full) {
-      *reinterpret_cast<int4*>(vals + first) = make_int4(o[0], o[1], o[2], o[3]);
-      *reinterpret_cast<int4*>(vals + first + 4) = make_int4(o[4], o[5], o[6], o[7]);
+#pragma unroll
+      for (int q = 0; q < kItems / 4; ++q)
+        *reinterpret_cast<int4*>(vals + first + 4 * q) = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
     } else {
 #pragma unroll
       for (int u = 0; u < kItems; ++u)
-        if (first + u < count) vals[first + u] = o[u];
+        if (first + u < count) vals[first + u] = v[u];
     }
     __syncthreads();
     if (threadIdx.x == blockDim.x - 1) carry = run;
