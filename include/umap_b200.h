@@ -126,7 +126,9 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     umapb_nnd_iteration (FP16 dot rounded when half != 0; FP32
  *                     rows need dd % 4 == 0).  *evals (nullable) += dots computed.
  *                     Sources are taken in the order of `order` (nullable, a
- *                     permutation; for cache locality only).
+ *                     permutation; for cache locality only).  With mc == k its
+ *                     buckets are the reverse-candidate buckets: rev_out
+ *                     (nullable) then receives what umapb_nnd_reverse would write.
  * umapb_nnd_sqrt:     Euclidean distances sqrt(max(d2, 0)) (nndescent.py:400).
  * umapb_nnd_random_start: the reference's random start drawn on the device
  *                     (nndescent.py:47-57, 72-82): from the NumPy legacy state in
@@ -151,7 +153,8 @@ int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, vo
 int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t* bytes);
 int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
                    const int32_t* order, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf, float* curd,
-                   unsigned long long* evals, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
+                   int32_t* rev_out, unsigned long long* evals, void* workspace, size_t workspace_bytes,
+                   umapb_stream_t stream);
 int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
                         const float* dist_old, const uint8_t* flags_old, const int32_t* rev, const int32_t* order,
                         const float* nnbuf, const float* curd, int64_t n, int32_t k,

@@ -192,13 +192,13 @@ class NNDescent:
         for it in range(self.n_iters):
             mc_nn, j_nn, mc_conv = iteration_params(update_frac, k, mc)
             use_rev = update_frac >= 0.10
-            if use_rev:
-                call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
             changed.zero_()
             evals.zero_()
             ev = self._events()
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
+                if use_rev:
+                    call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
                 ev[0].record() if ev else None
                 call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
                      ptr(rev if use_rev else None), ptr(order), ptr(None), ptr(None), n, k, mc_conv, j_nn, 1, 0,
@@ -236,10 +236,16 @@ class NNDescent:
                     nnbuf = torch.empty(n * k * k, dtype=torch.float32, device=dev)
                     curd = torch.empty((n, k), dtype=torch.float32, device=dev)
                     join_ws = _lib.workspace(query("umapb_nnd_join_workspace", n, k, k), dev)
+                # with every neighbour a source (mc_nn == k) the join's per-source
+                # buckets are the reverse-candidate buckets: it writes rev itself
+                rev_in_join = join and use_rev and mc_nn == k
+                if use_rev and not rev_in_join:
+                    call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
                 ev[0].record() if ev else None
                 if join:
                     call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(order), n, k,
-                         mc_nn, j_nn, ptr(nnbuf), ptr(curd), ptr(evals), ptr(join_ws), join_ws.numel(), s)
+                         mc_nn, j_nn, ptr(nnbuf), ptr(curd), ptr(rev if rev_in_join else None), ptr(evals),
+                         ptr(join_ws), join_ws.numel(), s)
                 call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
                      ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None),
                      ptr(curd if join else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),

@@ -199,16 +199,20 @@ __global__ void bucket_fill_kernel(const int32_t* __restrict__ idx, int64_t m, i
   }
 }
 
-// rev[j][p] = p-th smallest source in j's bucket, 0 when the bucket is shorter
+// rev[j][p] = p-th smallest source in j's bucket, 0 when the bucket is shorter.
+// Bucket entries hold the source row shifted left by `shift` bits (0 for the
+// reverse buckets, 5 for the join's (row, position) entries); deg == nullptr
+// takes the bucket sizes from the offsets (off[n] = total).
 __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const int32_t* __restrict__ off,
-                                     const int32_t* __restrict__ deg, int64_t n, int k, int32_t* __restrict__ rev) {
+                                     const int32_t* __restrict__ deg, int64_t n, int k, int shift,
+                                     int32_t* __restrict__ rev) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t j = (int64_t)blockIdx.x * kWarps + warp;
   if (j >= n) return;
-  const int cnt = deg[j];
+  const int cnt = deg ? deg[j] : off[j + 1] - off[j];
   const int32_t* b = bucket + off[j];
   if (cnt <= 32 && k <= 32) {  // the common case (mean in-degree k): one warp-wide bitonic sort
-    int v = lane < cnt ? b[lane] : 0x7fffffff;
+    int v = lane < cnt ? (b[lane] >> shift) : 0x7fffffff;
     for (int size = 2; size <= 32; size <<= 1) {
       for (int stride = size >> 1; stride > 0; stride >>= 1) {
         const int o = __shfl_xor_sync(0xffffffffu, v, stride);
@@ -232,7 +236,7 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
     } else {
       int best = 0x7fffffff;
       for (int t = lane; t < cnt; t += 32) {
-        const int s = b[t];
+        const int s = b[t] >> shift;
         if (s > prev && s < best) best = s;
       }
 #pragma unroll
@@ -242,7 +246,7 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
         return;
       }
       int c = 0;
-      for (int t = lane; t < cnt; t += 32) c += b[t] == best ? 1 : 0;
+      for (int t = lane; t < cnt; t += 32) c += (b[t] >> shift) == best ? 1 : 0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
       out = best;
@@ -980,7 +984,7 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n, total);
   nnd::bucket_fill_kernel<<<blocks, 256, 0, stream>>>(idx, m, k, off, fill, bucket);
   nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
-                                                                                                  n, k, rev);
+                                                                                                  n, k, 0, rev);
   UMAPB_LAUNCH_CHECK("nnd_reverse kernels");
   count_launches(4);
   return UMAPB_OK;
@@ -1004,8 +1008,8 @@ extern "C" int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t
 extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
                               const int32_t* idx_old, const int32_t* order, int64_t n, int32_t k, int32_t mc,
                               int32_t j_nn, float* nnbuf,
-                              float* curd, unsigned long long* evals, void* workspace, size_t workspace_bytes,
-                              umapb_stream_t stream_) {
+                              float* curd, int32_t* rev_out, unsigned long long* evals, void* workspace,
+                              size_t workspace_bytes, umapb_stream_t stream_) {
   clear_error();
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(Xd && sqd && idx_old, "nnd_join: null array argument");
@@ -1014,6 +1018,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   UMAPB_REQUIRE(k >= 1 && k <= 32, "nnd_join: k must be in [1, 32]");
   UMAPB_REQUIRE(mc >= 0 && mc <= k && j_nn >= 0 && j_nn <= k, "nnd_join: bad mc / j_nn");
   UMAPB_REQUIRE(!(mc > 0 && j_nn > 0) || nnbuf, "nnd_join: nnbuf is null");
+  UMAPB_REQUIRE(!rev_out || mc == k, "nnd_join: reverse candidates from the join need mc == k");
   if (half)
     UMAPB_REQUIRE(ldx % 8 == 0 && (reinterpret_cast<uintptr_t>(Xd) & 15) == 0,
                   "nnd_join: FP16 rows need a pitch that is a multiple of 8 and a 16-byte aligned base");
@@ -1040,6 +1045,10 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off);
   scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n + 1, total);
   nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off, fill, entries);
+  if (rev_out) {  // with mc == k the buckets are the reverse-candidate buckets
+    nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(
+        entries, off, nullptr, n, k, 5, rev_out);
+  }
   const unsigned sblocks = (unsigned)ceil_div(n, 256);
   UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
   nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, order, n, choff);
@@ -1079,7 +1088,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
     nnd::join_f32_kernel<<<jb, nnd::kWarps * 32, jsmem, stream>>>(a);
   }
   UMAPB_LAUNCH_CHECK("nnd_join kernels");
-  count_launches(7);
+  count_launches(rev_out ? 8 : 7);
   return UMAPB_OK;
 }
 

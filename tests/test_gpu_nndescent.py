@@ -156,7 +156,7 @@ def test_build_leaves_numpy_stream_like_the_reference():
 
 @pytest.mark.parametrize("half", [False, True])
 @pytest.mark.parametrize("n,d,k,mc,j_nn", [(3000, 64, 15, 15, 15), (1000, 784, 15, 9, 7), (517, 36, 32, 20, 32),
-                                           (40, 8, 5, 3, 2)])
+                                           (40, 8, 5, 3, 2), (333, 12, 6, 6, 4), (700, 40, 33 - 1, 32, 16)])
 def test_join_block_distances(n, d, k, mc, j_nn, half):
     """umapb_nnd_join: nnbuf[i][p*j_nn + j] = d(i, idx[idx[i][p]][j]) and curd[i][p] =
     d(i, idx[i][p]) with the iteration's distance rule (FP16 dots rounded to FP16)."""
@@ -184,8 +184,13 @@ def test_join_block_distances(n, d, k, mc, j_nn, half):
     ws = _lib.workspace(_lib.query("umapb_nnd_join_workspace", n, k, mc), Xd.device)
     # sources taken in a shuffled order: a scheduling choice that changes no output
     order = torch.from_numpy(rng.permutation(n).astype(np.int32)).cuda() if n % 2 else None
+    # with mc == k the join's buckets also give the reverse candidates
+    rev = torch.full((n, k), -7, dtype=torch.int32, device="cuda") if mc == k else None
     _lib.call("umapb_nnd_join", _lib.ptr(src), _lib.ptr(sq), d, ldx, int(half), _lib.ptr(d_idx), _lib.ptr(order), n,
-              k, mc, j_nn, _lib.ptr(nnbuf), _lib.ptr(curd), _lib.ptr(evals), _lib.ptr(ws), ws.numel(), s)
+              k, mc, j_nn, _lib.ptr(nnbuf), _lib.ptr(curd), _lib.ptr(rev), _lib.ptr(evals), _lib.ptr(ws), ws.numel(),
+              s)
+    if rev is not None:
+        assert np.array_equal(rev.cpu().numpy(), onnd.reverse_candidates(idx))
     got_nn, got_cur = nnbuf.cpu().numpy(), curd.cpu().numpy()
     assert int(evals.item()) == n * mc * (1 + j_nn)
     sqh = sq.cpu().numpy().astype(np.float64)
