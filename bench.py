@@ -11,18 +11,24 @@ offline), NNDescent k=15 with the reference's defaults (n_iters 20, delta
   fit_s   seconds per fit (the other half of the metric)
   e2e     the same metric through UMAP.fit_transform on a pinned host tensor,
           host->device input and device->host embedding copies inside the timing
-  roofline  the layout epoch (sgd_epoch_kernel + apply_kernel), the largest
-          kernel share of a fit: 112 algorithmic bytes per active edge over the
-          layout stage's CUDA-event time divided by the epochs
+  roofline  the layout epoch (one fused sgd_epoch_kernel launch per epoch), the
+          largest kernel share of a fit: 112 algorithmic bytes per active edge
+          over the layout stage's CUDA-event time divided by the epochs
   roofline_nndescent  one NNDescent iteration (join + row kernel), CUDA events
           around each launch in the timed fits, against two byte counts: every
           reference candidate row read once, and the rows the blocked join reads
-  cpu_baseline  the NumPy oracle of the reference algorithm on the host cores,
-          on a bounded sample of the workload, extrapolated per stage
+  knn_brute  the 20000 x 784 exact-kNN workload (untimed record): its three
+          launches timed with CUDA events, tile kernel against the BF16 peak
+  learned_init  layout epochs the learned warm start needs to reach the
+          500-epoch spectral trustworthiness (untimed record)
+  cpu_baseline  the NumPy port of the reference algorithm on the host cores, the
+          70,000-row workload at full size with each stage's work units sampled
+          (oracle.pipeline.FitSampler)
 
 N > 1 (torchrun): every rank fits its own replica (weak scaling, no
 collective on the data path); time = max over ranks.
-`--impl reference` times the reference algorithm's CPU port the same way.
+`--impl reference` times the reference algorithm's CPU port: each step one
+sampled full-size fit of FitSampler, rank 0 only.
 """
 
 from __future__ import annotations
@@ -44,7 +50,6 @@ sys.path.insert(0, HERE)
 
 METRIC = "UMAP fit s & edges/s @70K×784"
 N_FULL, D, K_NN, N_EPOCHS = 70000, 784, 15, 500
-CPU_SAMPLE_N = 2000
 
 
 def parse():
@@ -55,6 +60,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_FULL, help="rows (default: the 70K workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the untimed brute-kNN and learned-init records of the fit line")
     ap.add_argument("--case", choices=["fit", "learned_init", "scale", "nndescent", "knn_brute", "layout",
                                        "encoder"], default="fit",
                     help="fit: the benchmark line; learned_init: epochs-to-trustworthiness of the learned warm start; "
@@ -193,6 +200,16 @@ def measured_peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def measured_bf16_peak():
+    """Dense BF16 TFLOP/s (burst: kernels timed alone)."""
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
 
 
 def committed_traffic(name: str = "nnd_iteration_70k.md"):
@@ -381,7 +398,12 @@ def run_ours(args, rank, world, local_rank):
                        "wall_ms_per_step": round(e2e_wall, 2), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                "gpu_launches": launches, "gpu_launches_per_step": launches // args.steps,
                "clocks": clocks}
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_extras and world == 1:
+            # untimed records after the timed region: the brute-force kNN workload
+            # (20000 x 784) and the learned warm start against plain init
+            out["knn_brute"] = knn_brute_record(torch)
+            out["learned_init"] = learned_init_record(torch, X)
+        if not args.no_cpu_baseline and world == 1 and n == N_FULL:
             out["cpu_baseline"] = cpu_baseline()
     if dist is not None:
         dist.barrier()
@@ -389,15 +411,96 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
-def cpu_baseline():
-    from oracle.pipeline import estimate_fit
+def knn_brute_record(torch):
+    """umapb_knn_brute on the 20000 x 784 exact-kNN workload (k = 15, 31 candidates
+    reranked), the three launches timed with CUDA events (median of 5 calls after 2
+    warm-up calls): roofline of the tensor-core tile kernel on 2 n^2 d FLOPs."""
+    from mlx_vis_b200 import _lib
+    from mlx_vis_b200.datasets import prototype_mixture
 
-    r = estimate_fit(N_FULL, make_data, CPU_SAMPLE_N, n_epochs=N_EPOCHS, k=K_NN)
-    return {"value": r["edge_updates_full"] / r["fit_s_full"], "unit": "edges/s", "fit_s": round(r["fit_s_full"], 2),
-            "cores": r["threads"], "kind": "port",
-            "sample": r["sample"] + f"; extrapolated to {N_FULL} rows per stage (NNDescent, fuzzy set and spectral "
-                                    "init by rows, layout by positive-edge updates)",
-            "stage_s": {k: round(v, 2) for k, v in r["stage_s_full"].items()}, "cpu_s": round(r["cpu_s"], 2)}
+    n = 20000
+    Xd = torch.from_numpy(prototype_mixture(n, D, seed=0)).cuda()
+    runs = [_lib.knn_brute_timed(Xd, K_NN, extra=16)[2] for _ in range(7)][2:]
+    med = [statistics.median(r[i] for r in runs) for i in range(3)]
+    peak, src = measured_bf16_peak()
+    flops = 2.0 * n * n * D
+    call_ms = sum(med)
+    return {"workload": f"{n}x{D} prototype mixture, k={K_NN}, BF16 tcgen05 tiles + FP32 rerank of {K_NN + 16}",
+            "stage_ms": {"prep": round(med[0], 4), "tiles": round(med[1], 4), "rerank": round(med[2], 4)},
+            "call_ms": round(call_ms, 4), "bound": "tensor", "unit": "TFLOP/s", "peak": peak, "peak_source": src,
+            "achieved_tiles": round(flops / (med[1] * 1e-3) / 1e12, 1),
+            "frac_tiles": round(flops / (med[1] * 1e-3) / 1e12 / peak, 3),
+            "achieved_call": round(flops / (call_ms * 1e-3) / 1e12, 1),
+            "frac_call": round(flops / (call_ms * 1e-3) / 1e12 / peak, 3)}
+
+
+LI_TRAIN_SETS, LI_EPOCHS = 8, (25, 50, 100, 200, 500)
+
+
+def learned_init_record(torch, X):
+    """The metric's second half on the benchmark's own 70K input: an encoder
+    784 -> 512 -> 512 -> 2 trained (by the library's kernels) on 8 seeded 20000 x 784
+    draws sharing the benchmark's prototypes (seeds 1..8), then layout epochs needed
+    by the learned start to reach, within 0.005, the trustworthiness@15 of 500
+    epochs from the spectral start (10,000-row sample)."""
+    from mlx_vis_b200 import UMAP
+    from mlx_vis_b200.datasets import prototype_mixture
+    from mlx_vis_b200.encoder import Encoder
+    from mlx_vis_b200.metrics import trustworthiness
+
+    t0 = time.perf_counter()
+    Xs = [prototype_mixture(20000, D, seed=j, proto_seed=0) for j in range(1, LI_TRAIN_SETS + 1)]
+    enc = Encoder.train_on_umap_runs(Xs, n_epochs=200, encoder_epochs=30, seed=0)
+    train_s = time.perf_counter() - t0
+    Xd = torch.from_numpy(X).cuda()
+    sub = np.random.default_rng(0).choice(X.shape[0], 10000, replace=False)
+    curves = {}
+    for init in ("spectral", "learned"):
+        curves[init] = {}
+        for ne in LI_EPOCHS:
+            u = UMAP(n_epochs=ne, random_state=0, knn_method="nndescent", init=init, encoder=enc)
+            Y = u.fit_transform_device(Xd).cpu().numpy()
+            curves[init][ne] = {"trust": round(trustworthiness(X[sub], Y[sub], 15), 5),
+                                "fit_ms": round(u.timings_["total_device"], 2)}
+    ref = curves["spectral"][500]["trust"]
+    first = {tol: {init: next((ne for ne in LI_EPOCHS if curves[init][ne]["trust"] >= ref - tol), None)
+                   for init in ("spectral", "learned")} for tol in (0.005, 0.001)}
+    return {"workload": f"the benchmark's {X.shape[0]}x{D} input; encoder trained on {LI_TRAIN_SETS} x 20000x{D} "
+                        "draws with the same prototypes (200-epoch UMAP targets); trustworthiness@15 on 10,000 rows",
+            "train_s": round(train_s, 2), "spectral_500_trust": ref, "curves": curves,
+            "epochs_to_within_0.005": first[0.005], "epochs_to_within_0.001": first[0.001],
+            "learned_epoch_fraction_within_0.005": (None if first[0.005]["learned"] is None
+                                                    else first[0.005]["learned"] / 500)}
+
+
+_SAMPLER = None
+
+
+def fit_sampler():
+    """The reference algorithm's CPU port on the 70K workload (oracle.pipeline.FitSampler),
+    fed with the reference's own NNDescent graph and update log of this input
+    (tests/golden/c3_70k.npz)."""
+    global _SAMPLER
+    if _SAMPLER is None:
+        from mlx_vis_b200._curve import find_ab_params
+        from oracle.pipeline import FitSampler
+
+        g = np.load(os.path.join(HERE, "tests", "golden", "c3_70k.npz"))
+        a, b = find_ab_params(1.0, 0.1)
+        _SAMPLER = FitSampler(make_data(N_FULL), g["idx"], g["updates"], n_epochs=N_EPOCHS, a=a, b=b)
+    return _SAMPLER
+
+
+def cpu_baseline():
+    fs = fit_sampler()
+    t = time.perf_counter()
+    r = fs.step()
+    wall = time.perf_counter() - t
+    return {"value": fs.updates_total / r["fit"], "unit": "edges/s", "fit_s": round(r["fit"], 2),
+            "cores": fs.threads, "kind": "port", "sample": fs.describe(),
+            "stage_s": {k: round(v, 2) for k, v in r.items() if k != "fit"}, "cpu_s": round(wall, 2),
+            "reference_measured_here": "the reference's own modules on the NumPy mlx shim, the complete 70K fit, "
+                                       "measured once when the fixture was made: 508 s on 8 cores"}
 
 
 # --------------------------------------------------------------------------
@@ -568,16 +671,20 @@ def run_reference(args, rank):
         return None
     for _ in range(max(args.warmup, 3)):
         cpu_baseline()
-    vals, fits = [], []
+    vals, fits, stages = [], [], []
     t = time.perf_counter()
     for _ in range(args.steps):
         cb = cpu_baseline()
         vals.append(cb["value"])
         fits.append(cb["fit_s"])
-    ms = (time.perf_counter() - t) * 1e3 / args.steps
-    v = statistics.mean(vals)
+        stages.append(cb["stage_s"])
+    wall_ms = (time.perf_counter() - t) * 1e3 / args.steps
+    fit_s = statistics.mean(fits)
+    v = fit_sampler().updates_total / fit_s
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "edges/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": round(ms, 1), "fit_s": round(statistics.mean(fits), 2),
+            "warmup": max(args.warmup, 3), "ms_per_step": round(fit_s * 1e3, 1), "fit_s": round(fit_s, 2),
+            "sample_wall_ms_per_step": round(wall_ms, 1),
+            "stage_s": {k: round(statistics.mean(s[k] for s in stages), 2) for k in stages[0]},
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
             "data": "synthetic (seeded prototype mixture standing in for Fashion-MNIST)", "config": config(N_FULL),
             "cpu_baseline": {"value": v, "unit": "edges/s", "kind": "port", "cores": cb["cores"],

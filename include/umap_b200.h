@@ -47,6 +47,10 @@ unsigned long long umapb_kernel_launches(void);
 /* Synchronises `stream`, reads the device status word at `workspace` and
  * returns UMAPB_OK or UMAPB_ERR_DEVICE (with a message). */
 int umapb_read_status(const void* workspace, umapb_stream_t stream);
+/* Time limit in nanoseconds of the spectral power iteration's grid barrier, for
+ * launches made after the call (process-wide; 0 restores the default of 2 s).
+ * No counterpart in the reference, which has no device-side waits. */
+int umapb_set_wait_limit_ns(unsigned long long ns);
 
 /* ---------------------------------------------------------------------------
  * Exact brute-force kNN — replaces mlx_vis/_knn.py:47-88 (chunked
@@ -62,6 +66,23 @@ int umapb_knn_brute_workspace(int64_t n, int64_t d, int32_t k, int32_t extra, si
 int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
                     int32_t* out_idx, float* out_dist, void* workspace, size_t workspace_bytes,
                     umapb_stream_t stream);
+/* The same call with CUDA events between its three launches (operand prep, the
+ * tensor-core distance tiles with the fused top-(k+extra), the FP32 rerank);
+ * synchronises and writes the three stage times in milliseconds to stage_ms[3].
+ * For profiling; the results equal umapb_knn_brute's. */
+int umapb_knn_brute_timed(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                          int32_t* out_idx, float* out_dist, void* workspace, size_t workspace_bytes,
+                          float* stage_ms, umapb_stream_t stream);
+/* The kNN of the query rows [row_begin, row_begin + row_count) of X against all
+ * n rows (self excluded): out_idx / out_dist (row_count, k), the same values as
+ * those rows of umapb_knn_brute.  The row split of the reference's chunked loop
+ * (mlx_vis/_knn.py:58-79) spread over GPUs: each rank takes one block of rows
+ * and the (n, k) result is gathered (mlx_vis_b200/_distributed.py). */
+int umapb_knn_brute_rows_workspace(int64_t n, int64_t d, int32_t k, int32_t extra, int64_t row_begin,
+                                   int64_t row_count, size_t* bytes);
+int umapb_knn_brute_rows(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                         int64_t row_begin, int64_t row_count, int32_t* out_idx, float* out_dist,
+                         void* workspace, size_t workspace_bytes, umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Allocation-free brute-force kNN.  No counterpart in the reference: an extra
@@ -198,9 +219,17 @@ int umapb_fuzzy(const int32_t* knn_idx, const float* knn_dist, int64_t n, int32_
  *   V0    (n, dim+1) float32 start block (the reference draws it from mx.random)
  *   noise (n, dim)   float32 N(0, 1e-4) draw added after the 10/max|e| scaling
  *   Y     (n, dim)   float32 output, min-max scaled to [0, 10] per column
- * Each power iteration is one CSR SpMV that also accumulates the FP64 Gram
- * matrix; orthonormalisation uses its Cholesky factor (the same Q as the
- * reference's modified Gram-Schmidt).
+ * 1 <= dim <= 32.  Each power iteration is one CSR SpMV that also accumulates
+ * the FP64 Gram matrix; orthonormalisation uses its Cholesky factor (the same Q
+ * as the reference's modified Gram-Schmidt).  For dim <= 4 all iterations run
+ * in one cooperative launch whose grid barrier is a bounded wait: when it gives
+ * up, the status word at the start of the workspace is non-zero and Y is not a
+ * valid embedding.
+ * umapb_spectral_fallback: the reference's fallback to a random start
+ * (umap.py:354-357) without a host round trip: if the status word of the
+ * spectral workspace is non-zero, Y (n, dim) is overwritten on the device with
+ * 0.01 * the N(0, 1) stream of umapb_normal_fill(seed); otherwise Y is kept.
+ * Enqueue it on the same stream right after umapb_spectral.
  * ------------------------------------------------------------------------- */
 /* Standard normal draws for the spectral start block V0 — stands in for
  * mx.random.normal((n, c+1)) after mx.random.seed (umap.py:134-135, 325),
@@ -210,6 +239,8 @@ int umapb_spectral_workspace(int64_t n, int32_t dim, int64_t e_cap, int32_t n_it
 int umapb_spectral(const int32_t* rows, const int32_t* cols, const float* vals, const int64_t* n_edges,
                    int64_t e_cap, int64_t n, int32_t dim, const float* V0, int32_t n_iter, const float* noise,
                    float* Y, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
+int umapb_spectral_fallback(const void* workspace, float* Y, int64_t n, int32_t dim, uint64_t seed,
+                            umapb_stream_t stream);
 
 /* ---------------------------------------------------------------------------
  * Layout optimisation — replaces UMAP._optimize / _sgd_step
@@ -309,6 +340,41 @@ int umapb_adamw(int32_t n_groups, float* const* p, float* const* g, const int32_
                 void* const* p_bf16, const int32_t* ldb,
                 void* const* p_bf16_t, const int32_t* ldbt, float lr, float beta1, float beta2, float eps,
                 float weight_decay, const int32_t* step, umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Dense FP32 products on the BF16 tensor cores, column means and a key sort.
+ * Replace the reference's FP32 GEMMs of the NNDescent projections X @ P, X @ P2
+ * (mlx_vis/_nndescent/nndescent.py:72-82, 229-233) and of PCA (covariance and
+ * projection, mlx_vis/_umap/umap.py:92-111), and the row order NNDescent runs in.
+ * umapb_split3: operand rows for umapb_gemm_split3 from a row-major FP32 matrix S
+ *   (rows x cols, pitch lds), with the optional per-column mu subtracted: each
+ *   value x as three BF16 parts x0 + x1 + x2 (24 significant bits) at column
+ *   offsets 0, kp, 2 kp of an operand row of 3 kp BF16 (zero padded past K).
+ *   transpose == 0: operand row r = S row r (K = cols); != 0: operand row c =
+ *   S column c (K = rows).  kp: a multiple of 64, >= K.
+ * umapb_gemm_split3: C[m][n] = sum_k A[m][k] B[n][k] from split operands A3
+ *   (M x 3kp) and B3 (N x 3kp): six tcgen05 products per K block (x0y0, x0y1,
+ *   x1y0, x0y2, x2y0, x1y1) in one FP32 accumulator, error at FP32 level.  With
+ *   ksplit > 1 the K range is cut into slices, slice z written at C + z M ldc
+ *   (sum them with umapb_sum_slices).  *status (device int32) receives the
+ *   bounded-wait status.
+ * umapb_colmean: mean[c] over the rows (FP64 partial sums in a fixed order).
+ * umapb_sum_slices: out[t] = scale * sum_z C[z count + t].
+ * umapb_sort_keys: order = the stable ascending order of the n float keys
+ *   keys[0], keys[stride], ... (no NaN).
+ * ------------------------------------------------------------------------- */
+int umapb_split3(const float* S, int64_t rows, int64_t cols, int64_t lds, const float* mu, int32_t transpose,
+                 int32_t kp, void* out, umapb_stream_t stream);
+int umapb_gemm_split3(const void* A3, const void* B3, int32_t M, int32_t N, int32_t kp, int32_t ksplit, float* C,
+                      int32_t ldc, int32_t* status, umapb_stream_t stream);
+int umapb_colmean_workspace(int64_t rows, int64_t cols, size_t* bytes);
+int umapb_colmean(const float* S, int64_t rows, int64_t cols, int64_t lds, float* mean, void* workspace,
+                  size_t workspace_bytes, umapb_stream_t stream);
+int umapb_sum_slices(const float* C, int32_t slices, int64_t count, float scale, float* out, umapb_stream_t stream);
+int umapb_sort_keys_workspace(int64_t n, size_t* bytes);
+int umapb_sort_keys(const float* keys, int64_t n, int64_t stride, int32_t* order, void* workspace,
+                    size_t workspace_bytes,
+                    umapb_stream_t stream);
 
 #ifdef __cplusplus
 }

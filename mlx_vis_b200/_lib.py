@@ -27,14 +27,19 @@ SIGNATURES = {
     "umapb_last_error": [],
     "umapb_abi_version": [],
     "umapb_read_status": [_p, _p],
+    "umapb_set_wait_limit_ns": [_c.c_ulonglong],
     "umapb_knn_brute_workspace": [_i64, _i64, _i32, _i32, _psz],
     "umapb_knn_brute": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _sz, _p],
     "umapb_knn_brute_noalloc": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _p],
+    "umapb_knn_brute_timed": [_p, _i64, _i64, _i32, _i32, _i32, _p, _p, _p, _sz, _p, _p],
+    "umapb_knn_brute_rows_workspace": [_i64, _i64, _i32, _i32, _i64, _i64, _psz],
+    "umapb_knn_brute_rows": [_p, _i64, _i64, _i32, _i32, _i32, _i64, _i64, _p, _p, _p, _sz, _p],
     "umapb_fuzzy_workspace": [_i64, _i32, _psz],
     "umapb_fuzzy": [_p, _p, _i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _sz, _p],
     "umapb_normal_fill": [_p, _i64, _u64, _p],
     "umapb_spectral_workspace": [_i64, _i32, _i64, _i32, _psz],
     "umapb_spectral": [_p, _p, _p, _p, _i64, _i64, _i32, _p, _i32, _p, _p, _p, _sz, _p],
+    "umapb_spectral_fallback": [_p, _p, _i64, _i32, _u64, _p],
     "umapb_layout_workspace": [_i64, _i32, _i64, _psz],
     "umapb_layout_prepare": [_p, _p, _i64, _i32, _p, _p, _p, _sz, _p],
     "umapb_layout_epochs": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _f32, _f32, _f32, _i32,
@@ -65,6 +70,13 @@ SIGNATURES = {
     "umapb_legacy_normal_workspace": [_i64, _psz],
     "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p, _sz, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
+    "umapb_split3": [_p, _i64, _i64, _i64, _p, _i32, _i32, _p, _p],
+    "umapb_gemm_split3": [_p, _p, _i32, _i32, _i32, _i32, _p, _i32, _p, _p],
+    "umapb_colmean_workspace": [_i64, _i64, _psz],
+    "umapb_colmean": [_p, _i64, _i64, _i64, _p, _p, _sz, _p],
+    "umapb_sum_slices": [_p, _i32, _i64, _f32, _p, _p],
+    "umapb_sort_keys_workspace": [_i64, _psz],
+    "umapb_sort_keys": [_p, _i64, _i64, _p, _p, _sz, _p],
     "umapb_layout_epoch_injected": [_p, _i64, _i32, _p, _p, _p, _p, _p, _i64, _i32, _i32, _f32, _f32, _f32, _i32,
                                     _p, _i64, _p, _sz, _p],
 }
@@ -174,6 +186,37 @@ def knn_brute(X: torch.Tensor, k: int, extra: int = 16, squared: bool = False, c
     return idx, dist
 
 
+def knn_brute_rows(X: torch.Tensor, k: int, row_begin: int, row_count: int, extra: int = 16,
+                   squared: bool = False, check: bool = True):
+    """kNN of the rows [row_begin, row_begin + row_count) of X against all rows:
+    (idx int32 (row_count, k), dist float32 (row_count, k))."""
+    X = _require(X, torch.float32, 2, "X")
+    n, d = X.shape
+    ws = workspace(query("umapb_knn_brute_rows_workspace", n, d, k, extra, row_begin, row_count), X.device)
+    idx = torch.empty((row_count, k), dtype=torch.int32, device=X.device)
+    dist = torch.empty((row_count, k), dtype=torch.float32, device=X.device)
+    call("umapb_knn_brute_rows", ptr(X), n, d, k, extra, int(squared), row_begin, row_count, ptr(idx), ptr(dist),
+         ptr(ws), ws.numel(), stream_handle())
+    if check:
+        read_status(ws)
+    return idx, dist
+
+
+def knn_brute_timed(X: torch.Tensor, k: int, extra: int = 16):
+    """knn_brute with CUDA events between its launches: (idx, dist, [prep, tiles,
+    rerank] milliseconds); synchronises."""
+    X = _require(X, torch.float32, 2, "X")
+    n, d = X.shape
+    ws = workspace(query("umapb_knn_brute_workspace", n, d, k, extra), X.device)
+    idx = torch.empty((n, k), dtype=torch.int32, device=X.device)
+    dist = torch.empty((n, k), dtype=torch.float32, device=X.device)
+    ms = (_c.c_float * 3)()
+    call("umapb_knn_brute_timed", ptr(X), n, d, k, extra, 0, ptr(idx), ptr(dist), ptr(ws), ws.numel(),
+         _c.cast(ms, _c.c_void_p), stream_handle())
+    read_status(ws)
+    return idx, dist, [float(v) for v in ms]
+
+
 def fuzzy(knn_idx: torch.Tensor, knn_dist: torch.Tensor, n_epochs: int, fp64: bool = True,
           with_sigma: bool = False):
     """Fuzzy simplicial set: (rows, cols, vals, n_edges) with capacity n*k; n_edges is a
@@ -217,10 +260,19 @@ def legacy_normal(rs, shape, loc: float, scale: float, device, parallel: bool = 
     return out
 
 
+def set_wait_limit_ns(ns: int) -> None:
+    """Time limit of the spectral power iteration's grid barrier (0: the 2 s default)."""
+    call("umapb_set_wait_limit_ns", int(ns))
+
+
 def spectral(rows, cols, vals, n_edges, n: int, dim: int, V0: torch.Tensor, noise: torch.Tensor,
-             n_iter: int = 100, check: bool = False) -> torch.Tensor:
+             n_iter: int = 100, check: bool = False, fallback_seed=None, return_workspace: bool = False):
     """Spectral initial embedding (n, dim).  ``check`` synchronises and raises if
-    the power iteration's grid barrier gave up."""
+    the power iteration's grid barrier gave up.  With ``fallback_seed`` a failed
+    power iteration is replaced on the device by the random start
+    ``normal((n, dim), fallback_seed) * 0.01`` (umapb_spectral_fallback), with no
+    synchronisation; the workspace (returned with ``return_workspace``) holds the
+    status word that tells which one Y is."""
     V0 = _require(V0, torch.float32, 2, "V0")
     noise = _require(noise, torch.float32, 2, "noise")
     dev = V0.device
@@ -229,9 +281,17 @@ def spectral(rows, cols, vals, n_edges, n: int, dim: int, V0: torch.Tensor, nois
     Y = torch.empty((n, dim), dtype=torch.float32, device=dev)
     call("umapb_spectral", ptr(rows), ptr(cols), ptr(vals), ptr(n_edges), e_cap, n, dim, ptr(V0), int(n_iter),
          ptr(noise), ptr(Y), ptr(ws), ws.numel(), stream_handle())
+    if fallback_seed is not None:
+        call("umapb_spectral_fallback", ptr(ws), ptr(Y), n, dim, int(fallback_seed) & 0xFFFFFFFFFFFFFFFF,
+             stream_handle())
     if check:
         read_status(ws)
-    return Y
+    return (Y, ws) if return_workspace else Y
+
+
+def status_word(ws: torch.Tensor) -> int:
+    """The device status word at the start of a workspace (synchronises)."""
+    return int(ws[:4].view(torch.int32).item())
 
 
 class Layout:
@@ -271,6 +331,70 @@ class Layout:
              ptr(self.eps), ptr(self.next), ptr(self.n_edges), self.e_cap, int(epoch), self.n_epochs, float(a),
              float(b), float(learning_rate), int(neg_rate), ptr(neg_to), neg_to.numel(), ptr(self.ws),
              self.ws.numel(), stream_handle())
+
+
+def _kp(k: int) -> int:
+    return max(64, (int(k) + 63) // 64 * 64)
+
+
+def split3(S: torch.Tensor, mu=None, transpose: bool = False, kp: int | None = None):
+    """Split-precision operand rows of S (rows x cols, float32): S rows (K = cols) or,
+    with ``transpose``, S columns (K = rows), mu subtracted per stored column.
+    Returns (bf16 tensor (operand rows, 3 kp), kp)."""
+    S = _require(S, torch.float32, 2, "S")
+    rows, cols = S.shape
+    kp = _kp(rows if transpose else cols) if kp is None else int(kp)
+    out = torch.empty(((cols if transpose else rows), 3 * kp), dtype=torch.bfloat16, device=S.device)
+    if mu is not None:
+        mu = _require(mu, torch.float32, 1, "mu")
+    call("umapb_split3", ptr(S), rows, cols, S.stride(0), ptr(mu), int(bool(transpose)), kp, ptr(out),
+         stream_handle())
+    return out, kp
+
+
+def gemm_split3(A3: torch.Tensor, B3: torch.Tensor, kp: int, ksplit: int = 1, scale: float = 1.0,
+                status: torch.Tensor | None = None) -> torch.Tensor:
+    """C = A B^T (M x N, float32) from split operands (FP32-level products on tcgen05)."""
+    M, N = A3.shape[0], B3.shape[0]
+    dev = A3.device
+    st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
+    C = torch.empty((ksplit, M, N), dtype=torch.float32, device=dev)
+    call("umapb_gemm_split3", ptr(A3), ptr(B3), M, N, int(kp), int(ksplit), ptr(C), N, ptr(st), stream_handle())
+    if ksplit == 1 and scale == 1.0:
+        return C[0]
+    out = torch.empty((M, N), dtype=torch.float32, device=dev)
+    call("umapb_sum_slices", ptr(C), int(ksplit), M * N, float(scale), ptr(out), stream_handle())
+    return out
+
+
+def matmul(A: torch.Tensor, B: torch.Tensor, A3=None) -> torch.Tensor:
+    """A @ B for float32 A (M x K) and B (K x N) on the tensor cores with FP32-level
+    error (umapb_split3 + umapb_gemm_split3).  ``A3``: A already split (split3(A))."""
+    A3, kp = A3 if A3 is not None else split3(A)
+    B3, _ = split3(B, transpose=True, kp=kp)
+    return gemm_split3(A3, B3, kp)
+
+
+def colmean(S: torch.Tensor) -> torch.Tensor:
+    S = _require(S, torch.float32, 2, "S")
+    rows, cols = S.shape
+    ws = workspace(query("umapb_colmean_workspace", rows, cols), S.device)
+    mean = torch.empty(cols, dtype=torch.float32, device=S.device)
+    call("umapb_colmean", ptr(S), rows, cols, S.stride(0), ptr(mean), ptr(ws), ws.numel(), stream_handle())
+    return mean
+
+
+def sort_keys(keys: torch.Tensor) -> torch.Tensor:
+    """Stable ascending order (int32) of a float32 vector (strided views allowed,
+    e.g. one column of a row-major matrix)."""
+    if not isinstance(keys, torch.Tensor) or not keys.is_cuda or keys.dtype != torch.float32 or keys.dim() != 1:
+        raise ValueError("keys must be a 1-D float32 CUDA tensor")
+    n = keys.numel()
+    order = torch.empty(n, dtype=torch.int32, device=keys.device)
+    ws = workspace(query("umapb_sort_keys_workspace", n), keys.device)
+    call("umapb_sort_keys", _c.c_void_p(keys.data_ptr()), n, max(keys.stride(0), 1), ptr(order), ptr(ws), ws.numel(),
+         stream_handle())
+    return order
 
 
 def exported_symbols() -> list[str]:

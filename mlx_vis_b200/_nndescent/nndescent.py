@@ -19,10 +19,11 @@ The control flow is the reference's, kept on the host:
   (nndescent.py:103-220);
 * stop when the fraction of positional changes drops below delta (381-398).
 
-Every data-parallel step runs in libumap_b200 (nndescent.cu); the projections
-are plain FP32 GEMMs (cuBLAS through torch.matmul with TF32 disabled).  One
-device-to-host read per iteration fetches the change count that drives the
-control flow, as in the reference.
+Every data-parallel step runs in libumap_b200: the iterations in nndescent.cu,
+the projections X @ P and X @ P2 as split-precision tcgen05 GEMMs with
+FP32-level error (linalg.cu, gemm.cu), the locality order of the rows by the
+library's radix sort.  One device-to-host read per iteration fetches the change
+count that drives the control flow, as in the reference.
 """
 
 from __future__ import annotations
@@ -36,6 +37,12 @@ import torch
 from mlx_vis_b200 import _lib
 from mlx_vis_b200._device import to_device_f32, to_host
 from mlx_vis_b200._lib import call, ptr, query, stream_handle
+
+# neighbours per row: up to 32 on the warp-per-row kernels with the blocked join,
+# 33..100 on the block-per-row kernels (nnd_wide.cu)
+MAX_K = 100
+JOIN_MAX_K = 32
+
 
 def iteration_params(update_frac: float, k: int, mc: int):
     """mc_nn, j_nn and the converging-path mc_new of nndescent.py:100-101, 107.
@@ -142,8 +149,8 @@ class NNDescent:
         if n < 2:
             raise ValueError("NNDescent needs at least 2 points")
         k = min(self.k, n - 1)
-        if k > 32:
-            raise ValueError("NNDescent on the GPU supports k <= 32")
+        if k > MAX_K:
+            raise ValueError(f"NNDescent on the GPU supports k <= {MAX_K}")
         mc = self.max_candidates or k
         dev = X.device
         _lib.load()
@@ -158,9 +165,12 @@ class NNDescent:
         call("umapb_nnd_sqnorms", ptr(X), n, d, 0, ptr(sq), s)
         call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
 
+        X3 = None
         if P is not None:
-            with _no_tf32():
-                X_low = (X @ P).contiguous()
+            # X @ P on the tensor cores with FP32-level error; X's split operand is
+            # kept for X @ P2 in iteration 1
+            X3 = _lib.split3(X)
+            X_low = _lib.matmul(X, P, A3=X3)
             sq_low = torch.empty(n, dtype=torch.float32, device=dev)
             call("umapb_nnd_sqnorms", ptr(X_low), n, X_low.shape[1], 0, ptr(sq_low), s)
         else:
@@ -170,7 +180,7 @@ class NNDescent:
         # locality order of the rows (sorted by one random-projection coordinate):
         # rows and sources that run side by side then share most of their
         # candidate rows in the L2 cache; it changes no result
-        order = torch.argsort(X_low[:, 0]).to(torch.int32) if n > 1 else None
+        order = _lib.sort_keys(X_low[:, 0]) if n > 1 else None
         rev = torch.empty((n, k), dtype=torch.int32, device=dev)
         rev_ws = _lib.workspace(query("umapb_nnd_reverse_workspace", n, k), dev)
         idx2 = torch.empty_like(idx)
@@ -209,8 +219,8 @@ class NNDescent:
                 if it == 0:
                     Xd, sqd = X_low, sq_low
                 elif it == 1 and P2_d is not None:
-                    with _no_tf32():
-                        Xd = (X @ P2_d).contiguous()
+                    Xd = _lib.matmul(X, P2_d, A3=X3 if X3 is not None else _lib.split3(X))
+                    X3 = None  # the split operand is not needed after the last projection
                     sqd = torch.empty(n, dtype=torch.float32, device=dev)
                     call("umapb_nnd_sqnorms", ptr(Xd), n, Xd.shape[1], 0, ptr(sqd), s)
                 else:
@@ -231,7 +241,7 @@ class NNDescent:
                         call("umapb_nnd_to_half", ptr(Xd), n, dd, ldx, ptr(src), s)
                 else:
                     src = Xd
-                join = join_on and mc_nn > 0 and (use_half or dd % 4 == 0)
+                join = join_on and k <= JOIN_MAX_K and mc_nn > 0 and (use_half or dd % 4 == 0)
                 if join and nnbuf is None:
                     nnbuf = torch.empty(n * k * k, dtype=torch.float32, device=dev)
                     curd = torch.empty((n, k), dtype=torch.float32, device=dev)
@@ -276,17 +286,6 @@ class NNDescent:
         out = torch.empty_like(dist)
         _sqrt_into(dist, out)
         return idx, out
-
-
-class _no_tf32:
-    """Keeps the projection GEMMs in full FP32, like the reference's X @ P."""
-
-    def __enter__(self):
-        self.prev = torch.backends.cuda.matmul.allow_tf32
-        torch.backends.cuda.matmul.allow_tf32 = False
-
-    def __exit__(self, *exc):
-        torch.backends.cuda.matmul.allow_tf32 = self.prev
 
 
 def _sqrt_into(d2: torch.Tensor, out: torch.Tensor) -> None:

@@ -85,6 +85,7 @@ class UMAP:
         self.encoder = encoder
         self.use_graph = use_graph
         self.embedding_ = None
+        self._spectral_ws = None
         self.timings_ = {}
         self.profile_kernels = False  # CUDA events around NNDescent iteration kernels (bench roofline)
 
@@ -97,8 +98,8 @@ class UMAP:
 
     def fit_transform_device(self, X, epoch_callback=None) -> torch.Tensor:
         """Like fit_transform but returns the CUDA tensor (no device-to-host copy)."""
-        if self.n_components < 1 or self.n_components > 4:
-            raise ValueError("n_components must be between 1 and 4")
+        if self.n_components < 1 or self.n_components > 32:
+            raise ValueError("n_components must be between 1 and 32")
         dev = device()
         ev = _Events(dev)
         if self.normalize:
@@ -149,6 +150,8 @@ class UMAP:
 
         if self.verbose:
             print("Initializing embedding...")
+        self._spectral_ws = None
+        self.init_used_ = self.init
         Y = self._init_embedding(Xd, rows, cols, vals, n_edges, n, seed, draws)
         ev.mark("init")
 
@@ -156,21 +159,37 @@ class UMAP:
         ev.mark("layout")
         self.timings_ = ev.finish()
         self.graph_info_ = {"n_edges": int(n_edges.item())}
+        if self._spectral_ws is not None and _lib.status_word(self._spectral_ws) != 0:
+            # the power iteration's bounded grid barrier gave up; the device already
+            # replaced Y by the random start (umap.py:354-357)
+            self.init_used_ = "random"
+            if self.verbose:
+                print("Spectral init failed (grid barrier timed out), used random initialization")
+        self._spectral_ws = None
         return Y
 
     # ------------------------------------------------------------------
     def _pca(self, Xd: torch.Tensor) -> torch.Tensor:
-        """Optional PCA (umap.py:92-111): covariance GEMM and eigh on the device."""
-        n = Xd.shape[0]
-        mean = Xd.mean(dim=0)
-        Xc = Xd - mean
-        cov = (Xc.T @ Xc) / (n - 1)
-        evals, evecs = torch.linalg.eigh(cov.double())
-        proj = evecs[:, -self.pca_dim:].flip(-1).float()
+        """Optional PCA (umap.py:92-113): column means, the covariance
+        (X - mean)^T (X - mean) / (n - 1) and the projection (X - mean) @ V on the
+        tensor cores (split-precision BF16 products with FP32-level error), the
+        eigendecomposition on the host in float64 (the reference also runs eigh on
+        the CPU, umap.py:98), V = the last pca_dim eigenvectors in reverse order."""
+        n, d = Xd.shape
+        mean = _lib.colmean(Xd)
+        XT3, kpn = _lib.split3(Xd, mu=mean, transpose=True)  # operand rows = features, K = samples
+        tiles = ((d + 127) // 128) ** 2
+        ksplit = max(1, min(16, 148 // max(tiles, 1)))
+        cov = _lib.gemm_split3(XT3, XT3, kpn, ksplit=ksplit, scale=1.0 / max(n - 1, 1))
+        del XT3
+        evals, evecs = np.linalg.eigh(to_host(cov).astype(np.float64))
+        proj = np.ascontiguousarray(evecs[:, -self.pca_dim:][:, ::-1], dtype=np.float32)
+        self.pca_eigenvalues_ = evals
         if self.verbose:
             ret = float(evals[-self.pca_dim:].sum() / evals.sum())
             print(f"Variance retained: {ret * 100:.1f}%")
-        return (Xc @ proj).contiguous()
+        X3 = _lib.split3(Xd, mu=mean)
+        return _lib.matmul(Xd, torch.from_numpy(proj).to(Xd.device), A3=X3)
 
     @staticmethod
     def _wait(x_ready, dev):
@@ -201,13 +220,18 @@ class UMAP:
             raise ValueError(f"unknown init {self.init!r}")
         try:
             V0, noise_d = draws if draws is not None else self._spectral_draws(n, seed, dev)
-            Y = _lib.spectral(rows, cols, vals, n_edges, n, c, V0, noise_d, n_iter=100)
+            # a power iteration whose grid barrier gives up is replaced on the device
+            # by the random start below (no host round trip); fit_transform reads the
+            # status word once the fit is done
+            Y, self._spectral_ws = _lib.spectral(rows, cols, vals, n_edges, n, c, V0, noise_d, n_iter=100,
+                                                 fallback_seed=seed, return_workspace=True)
             if self.verbose:
                 print("Using spectral initialization")
             return Y
         except _lib.UmapB200Error as e:  # the reference falls back to random init (umap.py:354-357)
             if self.verbose:
                 print(f"Spectral init failed ({e}), using random initialization")
+            self.init_used_ = "random"
             return _lib.normal((n, c), seed, dev) * 0.01
 
     def _optimize(self, rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback):

@@ -33,6 +33,9 @@ int check_cuda(const char* what) {
 }
 
 static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<unsigned long long> g_wait_limit_ns{2000000000ull};
+
+unsigned long long wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
 
 void count_launches(int k) { g_launches.fetch_add((unsigned long long)k, std::memory_order_relaxed); }
 
@@ -89,6 +92,12 @@ const char* umapb_last_error(void) { return umapb::g_msg; }
 int umapb_abi_version(void) { return 1; }
 
 unsigned long long umapb_kernel_launches(void) { return umapb::g_launches.load(std::memory_order_relaxed); }
+
+int umapb_set_wait_limit_ns(unsigned long long ns) {
+  umapb::clear_error();
+  umapb::g_wait_limit_ns.store(ns ? ns : 2000000000ull, std::memory_order_relaxed);
+  return UMAPB_OK;
+}
 
 int umapb_read_status(const void* workspace, umapb_stream_t stream) {
   umapb::clear_error();

@@ -60,6 +60,10 @@ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 int num_sms();  // cached multiProcessorCount of the current device
 
+// Time limit of the bounded device-side waits that take it as a parameter
+// (umapb_set_wait_limit_ns; 2 s by default).
+unsigned long long wait_limit_ns();
+
 // Device status word values written by kernels with bounded waits.
 enum DeviceStatus : int32_t {
   kDevOk = 0,

@@ -55,10 +55,20 @@ struct EpiArgs {
 };
 
 
-template <int EPI>
+// Split-precision products (NPAIR = 6): A and B hold three BF16 parts per value,
+// x = x0 + x1 + x2 (x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1)),
+// side by side at column offsets 0, kp and 2 kp of each row.  The K loop then runs
+// over (K block, part pair) with the pairs (0,0) (0,1) (1,0) (0,2) (2,0) (1,1),
+// every product accumulated in the same FP32 TMEM tile: the dropped terms are
+// below 2^-24 of |a||b|, so C carries FP32-level error.  Consecutive iterations
+// reuse the K block's A and B tiles from L2.
+__constant__ int8_t kPairA[6] = {0, 0, 1, 0, 2, 1};
+__constant__ int8_t kPairB[6] = {0, 1, 0, 2, 0, 1};
+
+template <int EPI, int NPAIR = 1>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int num_kb,
-                EpiArgs e, int32_t* __restrict__ status) {
+                EpiArgs e, int32_t* __restrict__ status, int kp = 0, int n_major = 0) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -68,11 +78,14 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  // this CTA's K blocks [kb0, kb1); the host sizes the slices so none is empty
-  const int per = (num_kb + gridDim.z - 1) / gridDim.z;
+  // n_major: blockIdx.x walks the N tiles, so CTAs launched together share an A tile in L2
+  const int m0 = (n_major ? blockIdx.y : blockIdx.x) * BM, n0 = (n_major ? blockIdx.x : blockIdx.y) * BN;
+  // this CTA's K iterations [kb0, kb1) (K blocks x part pairs); the host sizes the
+  // slices so none is empty
+  const int num_it = num_kb * NPAIR;
+  const int per = (num_it + gridDim.z - 1) / gridDim.z;
   const int kb0 = blockIdx.z * per;
-  const int kb1 = kb0 + per < num_kb ? kb0 + per : num_kb;
+  const int kb1 = kb0 + per < num_it ? kb0 + per : num_it;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -102,8 +115,14 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (!tc::mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
         uint8_t* sa = smem + s * STAGE_BYTES;
         tc::mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-        tc::tma_load_2d(sa, &tmA, &full[s], kb * BK, m0);
-        tc::tma_load_2d(sa + A_BYTES, &tmB, &full[s], kb * BK, n0);
+        int xa = kb * BK, xb = kb * BK;
+        if (NPAIR > 1) {
+          const int k = kb / NPAIR, pr = kb - k * NPAIR;
+          xa = kPairA[pr] * kp + k * BK;
+          xb = kPairB[pr] * kp + k * BK;
+        }
+        tc::tma_load_2d(sa, &tmA, &full[s], xa, m0);
+        tc::tma_load_2d(sa + A_BYTES, &tmB, &full[s], xb, n0);
       }
     }
   } else if (warp == 1) {
@@ -262,4 +281,44 @@ extern "C" int umapb_gemm_bf16(const void* A, const void* B, int32_t M, int32_t 
     default:
       return set_error(UMAPB_ERR_ARG, "gemm: unknown epilogue %d", epilogue);
   }
+}
+
+extern "C" int umapb_gemm_split3(const void* A3, const void* B3, int32_t M, int32_t N, int32_t kp, int32_t ksplit,
+                                 float* C, int32_t ldc, int32_t* status, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(A3 && B3 && C && status, "gemm_split3: null argument");
+  UMAPB_REQUIRE(M >= 1 && N >= 1 && kp >= gemm::BK && kp % gemm::BK == 0,
+                "gemm_split3: need M, N >= 1 and kp a positive multiple of 64");
+  UMAPB_REQUIRE((int64_t)kp * 3 < ((int64_t)1 << 31), "gemm_split3: kp too large");
+  UMAPB_REQUIRE(ldc >= N, "gemm_split3: ldc must be >= N");
+  UMAPB_REQUIRE(ksplit >= 1 && ksplit <= 64, "gemm_split3: ksplit must be in [1, 64]");
+  static bool attr[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr[dev]) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(gemm::gemm_kernel<gemm::EPI_F32, 6>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM),
+                   "gemm_split3: smem attribute");
+    attr[dev] = true;
+  }
+  CUtensorMap ta, tb;
+  int s;
+  const uint64_t w = (uint64_t)kp * 3;
+  if ((s = make_tmap_bf16_2d(&ta, A3, (uint64_t)M, w, w, gemm::BM, gemm::BK))) return s;
+  if ((s = make_tmap_bf16_2d(&tb, B3, (uint64_t)N, w, w, gemm::BN, gemm::BK))) return s;
+  const int num_kb = kp / gemm::BK;
+  const int num_it = num_kb * 6;
+  const int per = (int)ceil_div(num_it, ksplit);
+  const int slices = (int)ceil_div(num_it, per);
+  gemm::EpiArgs e{M, N, C, ldc, nullptr, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, (int64_t)M * ldc};
+  if (slices < ksplit)
+    UMAPB_CUDA_TRY(cudaMemsetAsync(C + slices * e.slice, 0, sizeof(float) * (size_t)(ksplit - slices) * e.slice,
+                                   stream),
+                   "gemm_split3: empty slices");
+  dim3 grid((unsigned)ceil_div(N, gemm::BN), (unsigned)ceil_div(M, gemm::BM), (unsigned)slices);
+  gemm::gemm_kernel<gemm::EPI_F32, 6><<<grid, gemm::THREADS, gemm::SMEM, stream>>>(ta, tb, num_kb, e, status, kp, 1);
+  UMAPB_LAUNCH_CHECK("gemm_split3 kernel launch");
+  count_launches(1);
+  return UMAPB_OK;
 }

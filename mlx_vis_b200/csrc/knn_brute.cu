@@ -73,6 +73,7 @@ struct Cfg {
 
 struct Plan {
   int64_t n, d, ld;
+  int64_t m, r0;  // query rows [r0, r0 + m) against all n rows (m = n, r0 = 0: every row)
   int k, L, lcap, num_kb, slots;
   bool pair;     // 256-row tiles on CTA pairs (cta_group::2)
   int rb_rows;   // query rows per row block: 256 (pair) or 128
@@ -102,8 +103,15 @@ static bool pairing_enabled() {
   return !(e && e[0] == '0' && e[1] == 0);
 }
 
-static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) {
+static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p, int64_t r0 = 0,
+                     int64_t m = -1) {
+  if (m < 0) m = n;
   if (n < 2) return set_error(UMAPB_ERR_ARG, "knn_brute: need n >= 2 (got %lld)", (long long)n);
+  if (r0 < 0 || m < 1 || r0 + m > n)
+    return set_error(UMAPB_ERR_ARG, "knn_brute: query rows [%lld, %lld) outside [0, %lld)", (long long)r0,
+                     (long long)(r0 + m), (long long)n);
+  p.m = m;
+  p.r0 = r0;
   if (d < 1) return set_error(UMAPB_ERR_ARG, "knn_brute: need d >= 1");
   if (k < 1 || k > n - 1) return set_error(UMAPB_ERR_ARG, "knn_brute: need 1 <= k <= n-1 (k=%d, n=%lld)", k, (long long)n);
   if (extra < 0) return set_error(UMAPB_ERR_ARG, "knn_brute: extra must be >= 0");
@@ -128,7 +136,7 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) 
   }
   if (!p.pair) g = num_sms();
   p.rb_rows = p.pair ? 2 * BM : BM;
-  p.row_blocks = ceil_div(n, p.rb_rows);
+  p.row_blocks = ceil_div(m, p.rb_rows);
   p.col_tiles = ceil_div(n, BN);
   p.cols_pad = p.col_tiles * BN;
   p.tiles = p.row_blocks * p.col_tiles;
@@ -144,8 +152,8 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p) 
   p.status = c.take<int32_t>(64);
   p.xa = c.take<__nv_bfloat16>((size_t)n * p.ld, 1024);
   p.xb = c.take<__nv_bfloat16>((size_t)n * p.ld, 1024);
-  p.cand_s = c.take<float>((size_t)n * p.slots * p.L);
-  p.cand_i = c.take<int32_t>((size_t)n * p.slots * p.L);
+  p.cand_s = c.take<float>((size_t)m * p.slots * p.L);
+  p.cand_i = c.take<int32_t>((size_t)m * p.slots * p.L);
   p.ws_bytes = c.bytes();
   return UMAPB_OK;
 }
@@ -244,7 +252,8 @@ template <int LCAP, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1)
     topk_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 int n, int num_kb, int64_t col_tiles, int64_t tiles, int slots,
-                int L, float* __restrict__ cand_s, int32_t* __restrict__ cand_i, int32_t* __restrict__ status) {
+                int L, float* __restrict__ cand_s, int32_t* __restrict__ cand_i, int32_t* __restrict__ status,
+                int m_rows, int r0) {
   using C = Cfg<LCAP, PAIR>;
   constexpr int STAGE_BYTES = C::kStageBytes;
   constexpr int RB = C::kRowsPerBlock;
@@ -491,7 +500,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       merge_pending();
       const int64_t row = rb * RB + (int64_t)rank * BM + r;
       const int64_t slot = cta - first_cta(rb * col_tiles, tiles, G);
-      if (row < n) {
+      if (row < m_rows) {
         float* cs = cand_s + (row * slots + slot) * L;
         int32_t* ci = cand_i + (row * slots + slot) * L;
 #pragma unroll
@@ -522,8 +531,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       tc::tc_fence_after();
       const int64_t row = rb * RB + (int64_t)rank * BM + r;
-      const bool row_ok = row < n;
-      const int self_col = row_ok ? (int)row : -1;
+      const bool row_ok = row < m_rows;
+      const int self_col = row_ok ? (int)(row + r0) : -1;
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
       // Admission cap of the first tile of a row block, where the empty list
       // would admit every column: per 32-column group the 4th smallest valid
@@ -612,7 +621,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     auto flush = [&](int64_t rb) {
       const int64_t row = rb * BM + r;
       const int64_t slot = cta - first_cta(rb * col_tiles, tiles, G);
-      if (row < n) {
+      if (row < m_rows) {
         float* cs = cand_s + (row * slots + slot) * L;
         int32_t* ci = cand_i + (row * slots + slot) * L;
         for (int e = 0; e < L; ++e) {
@@ -639,7 +648,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       tc::tc_fence_after();
       const int64_t row = rb * BM + r;
-      const bool row_ok = row < n;
+      const bool row_ok = row < m_rows;
+      const int self_col = (int)(row + r0);
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
       for (int ch = 0; ch < BN / 32; ++ch) {
@@ -651,7 +661,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int j = 0; j < 32; ++j) {
           const float s = v[j];
           const int col = col0 + j;
-          if (s < tau && row_ok && col != row && col < n) {
+          if (s < tau && row_ok && col != self_col && col < n) {
             int p = L - 1;
             while (p > 0) {
               const float prev = list_s[(p - 1) * BM + r];
@@ -723,7 +733,7 @@ constexpr int RR_WARPS = 8;
 __global__ void __launch_bounds__(RR_WARPS * 32)
     rerank_kernel(const float* __restrict__ X, int64_t n, int d, const float* __restrict__ cand_s,
                   const int32_t* __restrict__ cand_i, int slots, int L, int P, int PL, int k, int squared,
-                  int32_t* __restrict__ out_idx, float* __restrict__ out_dist) {
+                  int32_t* __restrict__ out_idx, float* __restrict__ out_dist, int64_t r0 = 0) {
   extern __shared__ uint8_t smem_raw[];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -749,7 +759,7 @@ __global__ void __launch_bounds__(RR_WARPS * 32)
   warp_bitonic(key, idx, P, lane);
   // exact squared distances of the best L candidates (direct form, FP32), four
   // candidates per pass so every lane keeps several independent loads in flight
-  const float* xr = X + row * d;
+  const float* xr = X + (r0 + row) * d;  // rows: the query range [r0, r0 + n)
   const bool vec = (d & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
   for (int e0 = 0; e0 < PL; e0 += 4) {
     int j[4];
@@ -828,6 +838,26 @@ static int set_smem_attr() {
   return UMAPB_OK;
 }
 
+// The rerank kernel's dynamic shared memory (2 P floats per warp) can exceed the
+// 48 KB default; the attribute is raised once per device (up to 200 KB).
+static int rerank_smem_attr(size_t smem) {
+  if (smem <= 48 * 1024) return UMAPB_OK;
+  if (smem > 200 * 1024)
+    return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute: candidate merge needs %zu bytes of shared memory", smem);
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  UMAPB_CUDA_TRY(cudaGetDevice(&dev), "knn_brute: cudaGetDevice");
+  if (dev < 0 || dev >= 64) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute: device index %d", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!done[dev]) {
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)),
+                   "knn_brute: rerank smem attribute");
+    done[dev] = true;
+  }
+  return UMAPB_OK;
+}
+
 static int64_t resident_pairs() {
   static std::mutex mu;
   static int64_t cached[64];
@@ -865,7 +895,8 @@ static int launch_topk(const Plan& p, const CUtensorMap& ta, const CUtensorMap& 
   int s = set_smem_attr<LCAP, false>();
   if (s) return s;
   topk_kernel<LCAP, false><<<(unsigned)p.grid, THREADS, Cfg<LCAP, false>::kSmem, stream>>>(
-      ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles, p.slots, p.L, p.cand_s, p.cand_i, p.status);
+      ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles, p.slots, p.L, p.cand_s, p.cand_i, p.status, (int)p.m,
+      (int)p.r0);
   UMAPB_LAUNCH_CHECK("knn_brute: topk kernel launch");
   return UMAPB_OK;
 }
@@ -886,7 +917,7 @@ static int launch_topk_pair(const Plan& p, const CUtensorMap& ta, const CUtensor
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   UMAPB_CUDA_TRY(cudaLaunchKernelEx(&cfg, topk_kernel<32, true>, ta, tb, (int)p.n, p.num_kb, p.col_tiles, p.tiles,
-                                    p.slots, p.L, p.cand_s, p.cand_i, p.status),
+                                    p.slots, p.L, p.cand_s, p.cand_i, p.status, (int)p.m, (int)p.r0),
                  "knn_brute: pair topk kernel launch");
   return UMAPB_OK;
 }
@@ -896,7 +927,8 @@ static int launch_topk_pair(const Plan& p, const CUtensorMap& ta, const CUtensor
 static int run_tiles(const Plan& p, cudaStream_t stream) {
   CUtensorMap ta, tb;
   int s;
-  if ((s = make_tmap_bf16_2d(&ta, p.xa, (uint64_t)p.n, (uint64_t)p.ld, (uint64_t)p.ld, BM, BK))) return s;
+  if ((s = make_tmap_bf16_2d(&ta, p.xa + p.r0 * p.ld, (uint64_t)p.m, (uint64_t)p.ld, (uint64_t)p.ld, BM, BK)))
+    return s;
   if ((s = make_tmap_bf16_2d(&tb, p.xb, (uint64_t)p.n, (uint64_t)p.ld, (uint64_t)p.ld, p.pair ? BN / 2 : BN, BK)))
     return s;
   if (p.pair) return launch_topk_pair(p, ta, tb, stream);
@@ -926,6 +958,39 @@ extern "C" int umapb_knn_brute_workspace(int64_t n, int64_t d, int32_t k, int32_
   return UMAPB_OK;
 }
 
+// The three stages of one call; with `ev` (4 events) each stage boundary is recorded.
+static int enqueue_knn(const float* X, int64_t n, int64_t d, int32_t k, int32_t squared, int32_t* out_idx,
+                       float* out_dist, const knn::Plan& p, cudaStream_t stream, cudaEvent_t* ev) {
+  int s;
+  const int P = knn::next_pow2(p.slots * p.L);
+  const int PL = knn::next_pow2(p.L);
+  const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);
+  if ((s = knn::rerank_smem_attr(smem))) return s;
+  UMAPB_CUDA_TRY(cudaMemsetAsync(p.status, 0, sizeof(int32_t), stream), "knn_brute: status reset");
+  UMAPB_CUDA_TRY(cudaMemsetAsync(p.cand_i, 0xFF, (size_t)p.m * p.slots * p.L * sizeof(int32_t), stream),
+                 "knn_brute: candidate reset");
+  if (ev) UMAPB_CUDA_TRY(cudaEventRecord(ev[0], stream), "knn_brute: event");
+  {
+    const int64_t warps = n;
+    const unsigned blocks = (unsigned)ceil_div(warps * 32, 256);
+    knn::prep_kernel<<<blocks, 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
+    UMAPB_LAUNCH_CHECK("knn_brute: prep kernel launch");
+  }
+  if (ev) UMAPB_CUDA_TRY(cudaEventRecord(ev[1], stream), "knn_brute: event");
+  if ((s = knn::run_tiles(p, stream))) return s;
+  if (ev) UMAPB_CUDA_TRY(cudaEventRecord(ev[2], stream), "knn_brute: event");
+  {
+    const unsigned blocks = (unsigned)ceil_div(p.m, knn::RR_WARPS);
+    knn::rerank_kernel<<<blocks, knn::RR_WARPS * 32, smem, stream>>>(X, p.m, (int)d, p.cand_s, p.cand_i, p.slots,
+                                                                      p.L, P, PL, k, squared, out_idx, out_dist,
+                                                                      p.r0);
+    UMAPB_LAUNCH_CHECK("knn_brute: rerank kernel launch");
+  }
+  if (ev) UMAPB_CUDA_TRY(cudaEventRecord(ev[3], stream), "knn_brute: event");
+  count_launches(3);
+  return UMAPB_OK;
+}
+
 extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
                                int32_t* out_idx, float* out_dist, void* workspace, size_t workspace_bytes,
                                umapb_stream_t stream_) {
@@ -938,37 +1003,58 @@ extern "C" int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, 
   if (!workspace || workspace_bytes < p.ws_bytes)
     return set_error(UMAPB_ERR_WORKSPACE, "knn_brute: workspace of %zu bytes, need %zu", workspace_bytes, p.ws_bytes);
   knn::make_plan(n, d, k, extra, workspace, p);
+  return enqueue_knn(X, n, d, k, squared, out_idx, out_dist, p, stream, nullptr);
+}
 
-  UMAPB_CUDA_TRY(cudaMemsetAsync(p.status, 0, sizeof(int32_t), stream), "knn_brute: status reset");
-  UMAPB_CUDA_TRY(cudaMemsetAsync(p.cand_i, 0xFF, (size_t)n * p.slots * p.L * sizeof(int32_t), stream),
-                 "knn_brute: candidate reset");
-  {
-    const int64_t warps = n;
-    const unsigned blocks = (unsigned)ceil_div(warps * 32, 256);
-    knn::prep_kernel<<<blocks, 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
-    UMAPB_LAUNCH_CHECK("knn_brute: prep kernel launch");
-  }
-  if ((s = knn::run_tiles(p, stream))) return s;
-  {
-    const int P = knn::next_pow2(p.slots * p.L);
-    const int PL = knn::next_pow2(p.L);
-    const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);
-    if (smem > 48 * 1024) {
-      static bool set = false;
-      if (!set) {
-        UMAPB_CUDA_TRY(cudaFuncSetAttribute(knn::rerank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)(200 * 1024)),
-                       "knn_brute: rerank smem attribute");
-        set = true;
-      }
-    }
-    const unsigned blocks = (unsigned)ceil_div(n, knn::RR_WARPS);
-    knn::rerank_kernel<<<blocks, knn::RR_WARPS * 32, smem, stream>>>(X, n, (int)d, p.cand_s, p.cand_i, p.slots,
-                                                                      p.L, P, PL, k, squared, out_idx, out_dist);
-    UMAPB_LAUNCH_CHECK("knn_brute: rerank kernel launch");
-  }
-  count_launches(3);
+extern "C" int umapb_knn_brute_rows_workspace(int64_t n, int64_t d, int32_t k, int32_t extra, int64_t row_begin,
+                                              int64_t row_count, size_t* bytes) {
+  clear_error();
+  if (!bytes) return set_error(UMAPB_ERR_ARG, "bytes is null");
+  knn::Plan p;
+  int s = knn::make_plan(n, d, k, extra, nullptr, p, row_begin, row_count);
+  if (s) return s;
+  *bytes = p.ws_bytes;
   return UMAPB_OK;
+}
+
+extern "C" int umapb_knn_brute_rows(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                                    int64_t row_begin, int64_t row_count, int32_t* out_idx, float* out_dist,
+                                    void* workspace, size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(X && out_idx && out_dist, "knn_brute_rows: null array argument");
+  knn::Plan p;
+  int s = knn::make_plan(n, d, k, extra, nullptr, p, row_begin, row_count);
+  if (s) return s;
+  if (!workspace || workspace_bytes < p.ws_bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "knn_brute_rows: workspace of %zu bytes, need %zu", workspace_bytes,
+                     p.ws_bytes);
+  knn::make_plan(n, d, k, extra, workspace, p, row_begin, row_count);
+  return enqueue_knn(X, n, d, k, squared, out_idx, out_dist, p, stream, nullptr);
+}
+
+extern "C" int umapb_knn_brute_timed(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
+                                     int32_t* out_idx, float* out_dist, void* workspace, size_t workspace_bytes,
+                                     float* stage_ms, umapb_stream_t stream_) {
+  clear_error();
+  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+  UMAPB_REQUIRE(X && out_idx && out_dist && stage_ms, "knn_brute_timed: null argument");
+  knn::Plan p;
+  int s = knn::make_plan(n, d, k, extra, nullptr, p);
+  if (s) return s;
+  if (!workspace || workspace_bytes < p.ws_bytes)
+    return set_error(UMAPB_ERR_WORKSPACE, "knn_brute: workspace of %zu bytes, need %zu", workspace_bytes, p.ws_bytes);
+  knn::make_plan(n, d, k, extra, workspace, p);
+  cudaEvent_t ev[4] = {};
+  for (int i = 0; i < 4; ++i) UMAPB_CUDA_TRY(cudaEventCreate(&ev[i]), "knn_brute_timed: event create");
+  s = enqueue_knn(X, n, d, k, squared, out_idx, out_dist, p, stream, ev);
+  if (s == UMAPB_OK) {
+    cudaError_t e = cudaEventSynchronize(ev[3]);
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = cudaEventElapsedTime(&stage_ms[i], ev[i], ev[i + 1]);
+    if (e != cudaSuccess) s = set_error(UMAPB_ERR_CUDA, "knn_brute_timed: %s", cudaGetErrorString(e));
+  }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+  return s;
 }
 
 // ---------------------------------------------------------------------------
@@ -1033,18 +1119,17 @@ extern "C" int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int
   if ((s = scratch_address(&scratch))) return s;
   knn::make_plan(n, d, k, extra, scratch, p);
 
+  const int P = knn::next_pow2(p.slots * p.L);
+  const int PL = knn::next_pow2(p.L);
+  const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);
+  if ((s = knn::rerank_smem_attr(smem))) return s;  // before any launch: a refusal leaves nothing enqueued
+
   UMAPB_CUDA_TRY(cudaMemsetAsync(p.status, 0, sizeof(int32_t), stream), "knn_brute_noalloc: status reset");
   UMAPB_CUDA_TRY(cudaMemsetAsync(p.cand_i, 0xFF, (size_t)n * p.slots * p.L * sizeof(int32_t), stream),
                  "knn_brute_noalloc: candidate reset");
   knn::prep_kernel<<<(unsigned)ceil_div(n * 32, 256), 256, 0, stream>>>(X, n, (int)d, (int)p.ld, p.xa, p.xb);
   UMAPB_LAUNCH_CHECK("knn_brute_noalloc: prep kernel launch");
   if ((s = knn::run_tiles(p, stream))) return s;
-  const int P = knn::next_pow2(p.slots * p.L);
-  const int PL = knn::next_pow2(p.L);
-  const size_t smem = (size_t)knn::RR_WARPS * 2 * P * sizeof(float);
-  if (smem > 48 * 1024)
-    return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute_noalloc: candidate merge needs %zu bytes of shared memory",
-                     smem);
   knn::rerank_kernel<<<(unsigned)ceil_div(n, knn::RR_WARPS), knn::RR_WARPS * 32, smem, stream>>>(
       X, n, (int)d, p.cand_s, p.cand_i, p.slots, p.L, P, PL, k, squared, out_idx, out_dist);
   UMAPB_LAUNCH_CHECK("knn_brute_noalloc: rerank kernel launch");

@@ -27,7 +27,10 @@
 #include <cuda_fp16.h>
 #include <math.h>
 
+#include <mutex>
+
 #include "common.cuh"
+#include "nnd_wide.cuh"
 #include "scan.cuh"
 
 namespace umapb {
@@ -927,15 +930,24 @@ extern "C" int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int3
                                 int32_t k, int32_t sort_rows, umapb_stream_t stream_) {
   clear_error();
   UMAPB_REQUIRE(X && sq && idx && dist, "nnd_gather: null array argument");
-  UMAPB_REQUIRE(n >= 1 && dd >= 1 && k >= 1 && k <= 32, "nnd_gather: need 1 <= k <= 32");
+  UMAPB_REQUIRE(n >= 1 && dd >= 1 && k >= 1 && k <= nnd_wide_max_k(), "nnd_gather: need 1 <= k <= %d",
+                nnd_wide_max_k());
+  if (k > 32)
+    return nnd_gather_wide(X, sq, n, dd, idx, dist, k, sort_rows, reinterpret_cast<cudaStream_t>(stream_));
   const size_t smem = (size_t)nnd::kWarps * dd * sizeof(float);
   UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_gather: row dimension too large");
-  static bool attr = false;
-  if (!attr) {
-    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::gather_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024),
-                   "nnd_gather: smem attribute");
-    attr = true;
+  {
+    static std::mutex mu;
+    static bool attr[64] = {false};
+    int dev = 0;
+    UMAPB_CUDA_TRY(cudaGetDevice(&dev), "nnd_gather: device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+      UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::gather_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024),
+                     "nnd_gather: smem attribute");
+      attr[dev] = true;
+    }
   }
   nnd::gather_rows_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, smem,
                             reinterpret_cast<cudaStream_t>(stream_)>>>(X, sq, n, dd, idx, dist, k, sort_rows);
@@ -1110,8 +1122,13 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
                 "nnd_iteration: FP16 rows need a pitch that is a multiple of 8 and a 16-byte aligned base");
   UMAPB_REQUIRE(half || ldx % 4 != 0 || dd % 4 != 0 || (reinterpret_cast<uintptr_t>(Xd) & 15) == 0,
                 "nnd_iteration: FP32 rows need a 16-byte aligned base");
-  UMAPB_REQUIRE(k >= 1 && k <= 32, "nnd_iteration: k must be in [1, 32]");
+  UMAPB_REQUIRE(k >= 1 && k <= nnd_wide_max_k(), "nnd_iteration: k must be in [1, %d]", nnd_wide_max_k());
   UMAPB_REQUIRE(mc_new >= 0 && mc_new <= k && j_nn >= 0 && j_nn <= k, "nnd_iteration: bad mc_new / j_nn");
+  if (k > 32) {  // one block per row; every candidate distance computed in the row kernel
+    UMAPB_REQUIRE(!nnbuf && !curd, "nnd_iteration: the blocked join serves k <= 32 only");
+    return nnd_iteration_wide(Xd, sqd, dd, ldx, half, idx_old, dist_old, flags_old, rev, n, k, mc_new, j_nn,
+                              converging, recompute_cur, idx_new, dist_new, flags_new, changed, evals, stream);
+  }
   nnd::IterArgs a;
   a.Xd = Xd;
   a.sqd = sqd;
@@ -1151,15 +1168,21 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.evals = evals;
   const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(ldx, half ? 2 : 4, a.tcap, a.hcap);
   UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_iteration: row dimension too large for shared memory");
-  static bool attr = false;
-  if (!attr) {
-    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024),
-                   "nnd_iteration: smem attribute");
-    UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024),
-                   "nnd_iteration: smem attribute");
-    attr = true;
+  {
+    static std::mutex mu;
+    static bool attr[64] = {false};
+    int dev = 0;
+    UMAPB_CUDA_TRY(cudaGetDevice(&dev), "nnd_iteration: device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+      UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024),
+                     "nnd_iteration: smem attribute");
+      UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::iter_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024),
+                     "nnd_iteration: smem attribute");
+      attr[dev] = true;
+    }
   }
   const unsigned blocks = (unsigned)ceil_div(n, nnd::kWarps);
   if (half)

@@ -24,8 +24,10 @@ namespace umapb {
 namespace spectral {
 
 constexpr int kBlock = 256;
-constexpr int kMaxCols = 5;  // n_components <= 4
-constexpr int kLanes = 2;    // lanes per row in the power iteration
+constexpr int kMaxCols = 5;   // the fused kernels: n_components <= 4
+constexpr int kLanes = 2;     // lanes per row in the power iteration
+constexpr int kWideCols = 33; // the warp-per-row kernels: n_components <= 32
+constexpr int kWideRows = 32; // rows per block in the warp-per-row SpMV
 
 __global__ void row_ptr_kernel(const int32_t* __restrict__ rows, const int64_t* __restrict__ n_edges, int64_t n,
                                int64_t* __restrict__ row_ptr) {
@@ -162,6 +164,138 @@ __global__ void spmv_gram_kernel(const float* __restrict__ Vin, const double* __
 }
 
 
+// ---- n_components 5..32: one warp per row, lane j holds column j (and j + 32) ----
+// Cholesky factor R of the kk x kk Gram matrix (pivots sqrt(g - sum r^2 + 1e-10),
+// the same expressions and summation order as chol_inverse) and its inverse, by the
+// whole block in shared memory.  g is overwritten with R (upper triangle).
+__device__ void chol_inverse_block(double* g, int kk, double* ri) {
+  for (int i = 0; i < kk; ++i) {
+    if (threadIdx.x == 0) {
+      double s = g[i * kk + i];
+      for (int p = 0; p < i; ++p) s -= g[p * kk + i] * g[p * kk + i];
+      g[i * kk + i] = sqrt(fmax(s, 0.0) + 1e-10);
+    }
+    __syncthreads();
+    for (int j = i + 1 + threadIdx.x; j < kk; j += blockDim.x) {
+      double s = g[i * kk + j];
+      for (int p = 0; p < i; ++p) s -= g[p * kk + i] * g[p * kk + j];
+      g[i * kk + j] = s / g[i * kk + i];
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < kk; j += blockDim.x) {  // column j of R^-1
+    for (int i = kk - 1; i >= 0; --i) {
+      double s = (i == j) ? 1.0 : 0.0;
+      for (int p = i + 1; p < kk; ++p) s -= (p > j ? 0.0 : g[i * kk + p] * ri[p * kk + j]);
+      ri[i * kk + j] = (i <= j) ? s / g[i * kk + i] : 0.0;
+    }
+  }
+  __syncthreads();
+}
+
+// q_j = sum_{i <= j} u_i Rinv[i][j] for the columns j = lane and lane + 32 of a warp's row
+__device__ __forceinline__ void apply_rinv_wide(double u0, double u1, const double* ri, int kk, int lane,
+                                                double& q0, double& q1) {
+  q0 = 0.0, q1 = 0.0;
+  for (int i = 0; i < kk; ++i) {
+    const double ui = __shfl_sync(0xffffffffu, i < 32 ? u0 : u1, i & 31);
+    if (lane < kk && i <= lane) q0 += ui * ri[i * kk + lane];
+    if (lane + 32 < kk && i <= lane + 32) q1 += ui * ri[i * kk + lane + 32];
+  }
+}
+
+// One power iteration for kk > kMaxCols: Vout = (W Vin) Rinv_in (W Vin in FP64 per
+// row, one warp per row), G_out += Vout^T Vout from the block's rows staged in
+// shared memory; the last block factors G_out into Rinv_out.
+__global__ void __launch_bounds__(kBlock) spmv_gram_wide_kernel(
+    const float* __restrict__ Vin, const double* __restrict__ Rinv_in, const int64_t* __restrict__ row_ptr,
+    const int32_t* __restrict__ cols, const float* __restrict__ wn, int64_t n, int kk, int vp,
+    float* __restrict__ Vout, double* __restrict__ G_out, unsigned* __restrict__ counter,
+    double* __restrict__ Rinv_out) {
+  __shared__ double ri[kWideCols * kWideCols];
+  __shared__ double gl[kWideCols * kWideCols];
+  __shared__ double vs[kWideRows][kWideCols];
+  __shared__ bool last;
+  for (int t = threadIdx.x; t < kk * kk; t += blockDim.x)
+    ri[t] = Rinv_in ? Rinv_in[t] : ((t % (kk + 1) == 0) ? 1.0 : 0.0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t rb = (int64_t)blockIdx.x * kWideRows;
+  for (int lr = warp; lr < kWideRows; lr += kBlock / 32) {
+    const int64_t r = rb + lr;
+    double u0 = 0.0, u1 = 0.0;
+    if (r < n) {
+      const int64_t e1 = row_ptr[r + 1];
+      for (int64_t e = row_ptr[r]; e < e1; ++e) {
+        const int64_t c = cols[e];
+        const double w = (double)wn[e];
+        if (lane < kk) u0 += w * (double)Vin[c * vp + lane];
+        if (lane + 32 < kk) u1 += w * (double)Vin[c * vp + lane + 32];
+      }
+    }
+    double q0, q1;
+    apply_rinv_wide(u0, u1, ri, kk, lane, q0, q1);
+    if (r < n) {
+      if (lane < vp) Vout[r * vp + lane] = lane < kk ? (float)q0 : 0.f;
+      if (lane + 32 < vp) Vout[r * vp + lane + 32] = lane + 32 < kk ? (float)q1 : 0.f;
+    }
+    vs[lr][lane] = (r < n && lane < kk) ? q0 : 0.0;
+    if (lane + 32 < kWideCols) vs[lr][lane + 32] = (r < n && lane + 32 < kk) ? q1 : 0.0;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kk * kk; t += blockDim.x) {
+    const int i = t / kk, j = t % kk;
+    if (i <= j) {
+      double g = 0.0;
+      for (int lr = 0; lr < kWideRows; ++lr) g += vs[lr][i] * vs[lr][j];
+      atomicAdd(&G_out[i * kk + j], g);
+      if (i != j) atomicAdd(&G_out[j * kk + i], g);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int t = threadIdx.x; t < kk * kk; t += blockDim.x) gl[t] = __ldcg(G_out + t);
+  __syncthreads();
+  chol_inverse_block(gl, kk, ri);
+  for (int t = threadIdx.x; t < kk * kk; t += blockDim.x) Rinv_out[t] = ri[t];
+}
+
+// embedding = (V R^-1)[:, 1:] and max |embedding| for kk > kMaxCols (one warp per row)
+__global__ void __launch_bounds__(kBlock) finish_orth_wide_kernel(const float* __restrict__ V,
+                                                                  const double* __restrict__ Rinv, int64_t n, int kk,
+                                                                  int vp, float* __restrict__ emb,
+                                                                  unsigned* __restrict__ absmax) {
+  __shared__ double ri[kWideCols * kWideCols];
+  for (int t = threadIdx.x; t < kk * kk; t += blockDim.x) ri[t] = Rinv[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * (kBlock / 32) + warp;
+  float m = 0.f;
+  const double v0 = (r < n && lane < kk) ? (double)V[r * vp + lane] : 0.0;
+  const double v1 = (r < n && lane + 32 < kk) ? (double)V[r * vp + lane + 32] : 0.0;
+  double q0, q1;
+  apply_rinv_wide(v0, v1, ri, kk, lane, q0, q1);
+  if (r < n) {
+    if (lane >= 1 && lane < kk) {
+      const float f = (float)q0;
+      emb[r * (kk - 1) + (lane - 1)] = f;
+      m = fabsf(f);
+    }
+    if (lane + 32 < kk) {
+      const float f = (float)q1;
+      emb[r * (kk - 1) + (lane + 31)] = f;
+      m = fmaxf(m, fabsf(f));
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) atomicMax(absmax, __float_as_uint(m));
+}
+
 // ---- all power iterations in one cooperative launch ---------------------------
 // The per-iteration launches above spend most of their time starting and ending
 // (100 dependent launches of a few microseconds of work).  Here the grid stays
@@ -169,9 +303,9 @@ __global__ void spmv_gram_kernel(const float* __restrict__ Vin, const double* __
 // grid-stride range of rows, then one grid barrier, after which EVERY block
 // factors the completed Gram matrix itself (a few FP64 operations) instead of
 // waiting for a last block.  V rows written by other blocks are read through L2
-// (ld.global.cg).  The barrier gives up after kBarrierLimitNs, raises a shared
-// abort flag and the status word, and every block then returns.
-constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
+// (ld.global.cg).  The barrier gives up after limit_ns (umapb_set_wait_limit_ns,
+// 2 s by default), raises a shared abort flag and the status word, and every
+// block then returns.
 
 __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
@@ -179,7 +313,7 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
-__device__ bool grid_barrier(unsigned* bar, unsigned target, int* abort_g) {
+__device__ bool grid_barrier(unsigned* bar, unsigned target, int* abort_g, unsigned long long limit_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -191,16 +325,14 @@ __device__ bool grid_barrier(unsigned* bar, unsigned target, int* abort_g) {
       unsigned v;
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
       if (v >= target) break;
-      if ((i & 255) == 0) {
-        if (*(volatile int*)abort_g) {
-          ok = 0;
-          break;
-        }
-        if (gtimer() - t0 > kBarrierLimitNs) {
-          atomicExch(abort_g, 1);
-          ok = 0;
-          break;
-        }
+      if ((i & 255) == 0 && *(volatile int*)abort_g) {
+        ok = 0;
+        break;
+      }
+      if (gtimer() - t0 > limit_ns) {
+        atomicExch(abort_g, 1);
+        ok = 0;
+        break;
       }
     }
     __threadfence();
@@ -216,7 +348,8 @@ __global__ void __launch_bounds__(kBlock) power_kernel(float* __restrict__ V0, f
                                                        const int32_t* __restrict__ cols, const float* __restrict__ wn,
                                                        int64_t n, int n_iter, double* __restrict__ G,
                                                        double* __restrict__ Rinv, unsigned* __restrict__ bar,
-                                                       int* __restrict__ abort_g, int32_t* __restrict__ status) {
+                                                       int* __restrict__ abort_g, int32_t* __restrict__ status,
+                                                       unsigned long long limit_ns) {
   constexpr int kk = KK;
   constexpr int vp = KK <= 4 ? 4 : 8;
   __shared__ double ri[kMaxCols * kMaxCols];
@@ -289,7 +422,7 @@ __global__ void __launch_bounds__(kBlock) power_kernel(float* __restrict__ V0, f
         if (i != j) atomicAdd(&Git[j * kk + i], g);
       }
     }
-    if (!grid_barrier(bar, (unsigned)(it + 1) * gridDim.x, abort_g)) {
+    if (!grid_barrier(bar, (unsigned)(it + 1) * gridDim.x, abort_g, limit_ns)) {
       if (threadIdx.x == 0) atomicExch(status, (int32_t)kDevTimeoutEpilogue);
       return;
     }
@@ -374,11 +507,11 @@ struct Layout {
   unsigned* done;  // per-iteration block counters; done[n_iter] the grid barrier
   int* abort_g;    // cooperative path: barrier abort flag
   float* emb;
-  unsigned* red;  // absmax, colmin[4], colmax[4]
+  unsigned* red;  // absmax, colmin[kWideCols], colmax[kWideCols]
   size_t bytes;
 };
 
-static int vpitch(int kk) { return kk <= 4 ? 4 : 8; }
+static int vpitch(int kk) { return kk <= 4 ? 4 : (kk + 3) / 4 * 4; }
 
 static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   const int kk = dim + 1;
@@ -395,7 +528,7 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap, int n_iter) {
   l.done = c.take<unsigned>((size_t)(n_iter > 0 ? n_iter : 1) + 1);
   l.abort_g = c.take<int>(1);
   l.emb = c.take<float>((size_t)n * dim);
-  l.red = c.take<unsigned>(16);
+  l.red = c.take<unsigned>(1 + 2 * kWideCols);
   l.bytes = c.bytes();
   return l;
 }
@@ -411,16 +544,21 @@ __global__ void pad_rows_kernel(const float* __restrict__ a, int64_t n, int kk, 
 
 // Standard normal draws: element i of the stream (seed) comes from Philox block i/4
 // and the Box-Muller transform of its two 32-bit pairs.
-__global__ void normal_fill_kernel(float* __restrict__ out, int64_t count, uint32_t k0, uint32_t k1) {
-  const int64_t blk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (blk * 4 >= count) return;
+__device__ __forceinline__ void normal4(int64_t blk, uint32_t k0, uint32_t k1, float (&z)[4]) {
   const U4 r = philox4x32_10(U4{(uint32_t)blk, (uint32_t)(blk >> 32), 0x5eedu, 0u}, k0, k1);
   float s0, c0, s1, c1;
   const float r0 = sqrtf(-2.0f * logf(to_unit(r.x)));
   const float r1 = sqrtf(-2.0f * logf(to_unit(r.z)));
   sincospif(2.0f * to_unit(r.y), &s0, &c0);
   sincospif(2.0f * to_unit(r.w), &s1, &c1);
-  const float z[4] = {r0 * c0, r0 * s0, r1 * c1, r1 * s1};
+  z[0] = r0 * c0, z[1] = r0 * s0, z[2] = r1 * c1, z[3] = r1 * s1;
+}
+
+__global__ void normal_fill_kernel(float* __restrict__ out, int64_t count, uint32_t k0, uint32_t k1) {
+  const int64_t blk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk * 4 >= count) return;
+  float z[4];
+  normal4(blk, k0, k1, z);
   for (int u = 0; u < 4; ++u)
     if (blk * 4 + u < count) out[blk * 4 + u] = z[u];
 }
@@ -428,9 +566,25 @@ __global__ void normal_fill_kernel(float* __restrict__ out, int64_t count, uint3
 __global__ void init_red_kernel(unsigned* red, int dim) {
   if (threadIdx.x == 0) red[0] = 0u;
   if (threadIdx.x < (unsigned)dim) {
-    red[1 + threadIdx.x] = 0xFFFFFFFFu;  // min
-    red[5 + threadIdx.x] = 0u;           // max
+    red[1 + threadIdx.x] = 0xFFFFFFFFu;          // min
+    red[1 + kWideCols + threadIdx.x] = 0u;       // max
   }
+}
+
+// The reference falls back to a random start when its spectral init fails
+// (umap.py:354-357).  When the power iteration's grid barrier gave up (status word
+// non-zero), Y is replaced on the device by N(0, 1) * 0.01 drawn from the Philox
+// stream of umapb_normal_fill(seed), so no host round trip sits between the
+// spectral init and the layout.
+__global__ void fallback_kernel(const int32_t* __restrict__ status, float* __restrict__ Y, int64_t count,
+                                uint32_t k0, uint32_t k1) {
+  if (*status == 0) return;
+  const int64_t blk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (blk * 4 >= count) return;
+  float z[4];
+  normal4(blk, k0, k1, z);
+  for (int u = 0; u < 4; ++u)
+    if (blk * 4 + u < count) Y[blk * 4 + u] = __fmul_rn(z[u], 0.01f);
 }
 
 }  // namespace spectral
@@ -441,7 +595,7 @@ using namespace umapb;
 extern "C" int umapb_spectral_workspace(int64_t n, int32_t dim, int64_t e_cap, int32_t n_iter, size_t* bytes) {
   clear_error();
   UMAPB_REQUIRE(bytes, "bytes is null");
-  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4, "spectral: need n >= 1 and 1 <= dim <= 4");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 32, "spectral: need n >= 1 and 1 <= dim <= 32");
   UMAPB_REQUIRE(n_iter >= 1 && n_iter <= 128, "spectral: need 1 <= n_iter <= 128");
   UMAPB_REQUIRE(e_cap >= 0, "spectral: e_cap must be >= 0");
   *bytes = spectral::carve(nullptr, n, dim, e_cap, n_iter).bytes;
@@ -455,7 +609,7 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   clear_error();
   cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
   UMAPB_REQUIRE(rows && cols && vals && n_edges && V0 && noise && Y, "spectral: null array argument");
-  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 4, "spectral: need n >= 1 and 1 <= dim <= 4");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 32, "spectral: need n >= 1 and 1 <= dim <= 32");
   UMAPB_REQUIRE(n_iter >= 1 && n_iter <= 128, "spectral: need 1 <= n_iter <= 128");
   UMAPB_REQUIRE(e_cap >= 0, "spectral: e_cap must be >= 0");
   spectral::Layout l = spectral::carve(nullptr, n, dim, e_cap, n_iter);
@@ -500,6 +654,8 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   int64_t grid = (int64_t)num_sms() * (per_sm < 4 ? per_sm : 4);
   if (grid > (int64_t)pb) grid = pb;
   bool launched = false;
+  const bool wide = kk > spectral::kMaxCols;
+  if (wide) coop = 0;
   if (coop && grid > 0) {
     float* v0 = l.V[0];
     float* v1 = l.V[1];
@@ -512,12 +668,21 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
     unsigned* bar = l.done + n_iter;
     int* ab = l.abort_g;
     int32_t* st = l.status;
-    void* args[] = {&v0, &v1, &rp, &cols, &w, &nn, &ni, &G, &R, &bar, &ab, &st};
+    unsigned long long lim = wait_limit_ns();
+    void* args[] = {&v0, &v1, &rp, &cols, &w, &nn, &ni, &G, &R, &bar, &ab, &st, &lim};
     launched = cudaLaunchCooperativeKernel(pk, dim3((unsigned)grid), dim3(spectral::kBlock), args, 0, stream) ==
                cudaSuccess;
     if (!launched) cudaGetLastError();
   }
-  if (!launched) {
+  if (!launched && wide) {
+    const unsigned wb = (unsigned)ceil_div(n, spectral::kWideRows);
+    for (int it = 0; it < n_iter; ++it) {
+      const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
+      spectral::spmv_gram_wide_kernel<<<wb, spectral::kBlock, 0, stream>>>(
+          l.V[it & 1], rprev, l.row_ptr, cols, l.wn, n, kk, vp, l.V[(it + 1) & 1], l.G + (size_t)it * kk * kk,
+          l.done + it, l.Rinv + (size_t)it * kk * kk);
+    }
+  } else if (!launched) {
     for (int it = 0; it < n_iter; ++it) {
       const double* rprev = it == 0 ? nullptr : l.Rinv + (size_t)(it - 1) * kk * kk;
       spectral::spmv_gram_kernel<<<pb, spectral::kBlock, 0, stream>>>(
@@ -527,15 +692,34 @@ extern "C" int umapb_spectral(const int32_t* rows, const int32_t* cols, const fl
   }
   UMAPB_LAUNCH_CHECK("spectral: power iteration");
   spectral::init_red_kernel<<<1, 32, 0, stream>>>(l.red, dim);
-  spectral::finish_orth_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[n_iter & 1],
-                                                                     l.Rinv + (size_t)(n_iter - 1) * kk * kk, n,
-                                                                     kk, vp, l.emb, l.red);
+  if (wide)
+    spectral::finish_orth_wide_kernel<<<(unsigned)ceil_div(n, spectral::kBlock / 32), spectral::kBlock, 0, stream>>>(
+        l.V[n_iter & 1], l.Rinv + (size_t)(n_iter - 1) * kk * kk, n, kk, vp, l.emb, l.red);
+  else
+    spectral::finish_orth_kernel<<<rb, spectral::kBlock, 0, stream>>>(l.V[n_iter & 1],
+                                                                       l.Rinv + (size_t)(n_iter - 1) * kk * kk, n,
+                                                                       kk, vp, l.emb, l.red);
   const unsigned eb = (unsigned)ceil_div(n * dim, spectral::kBlock);
-  spectral::scale_noise_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, noise, n, dim, l.red, l.red + 1,
-                                                                     l.red + 5);
-  spectral::minmax_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, n, dim, l.red + 1, l.red + 5, Y);
+  unsigned* colmin = l.red + 1;
+  unsigned* colmax = l.red + 1 + spectral::kWideCols;
+  spectral::scale_noise_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, noise, n, dim, l.red, colmin, colmax);
+  spectral::minmax_kernel<<<eb, spectral::kBlock, 0, stream>>>(l.emb, n, dim, colmin, colmax, Y);
   UMAPB_LAUNCH_CHECK("spectral: rescale kernels");
   count_launches((e_cap > 0 ? 3 : 2) + 1 + (launched ? 1 : n_iter) + 4);
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_spectral_fallback(const void* workspace, float* Y, int64_t n, int32_t dim, uint64_t seed,
+                                       umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(workspace && Y, "spectral_fallback: null argument");
+  UMAPB_REQUIRE(n >= 1 && dim >= 1 && dim <= 32, "spectral_fallback: need n >= 1 and 1 <= dim <= 32");
+  const int64_t count = n * dim;
+  const int64_t blocks4 = ceil_div(count, 4);
+  spectral::fallback_kernel<<<(unsigned)ceil_div(blocks4, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream_)>>>(
+      static_cast<const int32_t*>(workspace), Y, count, (uint32_t)seed, (uint32_t)(seed >> 32));
+  UMAPB_LAUNCH_CHECK("spectral_fallback kernel");
+  count_launches(1);
   return UMAPB_OK;
 }
 

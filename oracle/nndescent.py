@@ -15,23 +15,39 @@ import numpy as np
 _BIG = np.float32(1e30)
 
 
+def _chunk_rows(c: int, d: int) -> int:
+    # rows per gather chunk: about 2^25 gathered values, so large k stays in memory;
+    # every row's dot products are independent, so chunking changes no value
+    return max(1, (1 << 25) // max(c * d, 1))
+
+
 def gather_d2(Xd: np.ndarray, sq: np.ndarray, cols: np.ndarray) -> np.ndarray:
     """_gather_dists (nndescent.py:573-612): max(sq_i + sq_c - 2 x_i.x_c, 0), float32."""
     n, c = cols.shape
-    flat = cols.reshape(-1)
-    dots = np.einsum("id,icd->ic", Xd, Xd[flat].reshape(n, c, Xd.shape[1]))
-    return np.maximum(sq[:, None] + sq[flat].reshape(n, c) - np.float32(2.0) * dots, np.float32(0))
+    out = np.empty((n, c), dtype=np.float32)
+    step = _chunk_rows(c, Xd.shape[1])
+    for s in range(0, n, step):
+        e = min(s + step, n)
+        flat = cols[s:e].reshape(-1)
+        dots = np.einsum("id,icd->ic", Xd[s:e], Xd[flat].reshape(e - s, c, Xd.shape[1]))
+        out[s:e] = np.maximum(sq[s:e, None] + sq[flat].reshape(e - s, c) - np.float32(2.0) * dots, np.float32(0))
+    return out
 
 
 def gather_d2_half(Xd: np.ndarray, sq: np.ndarray, cols: np.ndarray) -> np.ndarray:
     """_gather_dists_half (nndescent.py:615-641): float16 operands, the dot rounded to
     float16 (float32 accumulation), norms kept in float32."""
     n, c = cols.shape
-    flat = cols.reshape(-1)
     Xh = Xd.astype(np.float16).astype(np.float32)
-    dots = np.einsum("id,icd->ic", Xh, Xh[flat].reshape(n, c, Xd.shape[1]))
-    dots = dots.astype(np.float16).astype(np.float32)
-    return np.maximum(sq[:, None] + sq[flat].reshape(n, c) - np.float32(2.0) * dots, np.float32(0))
+    out = np.empty((n, c), dtype=np.float32)
+    step = _chunk_rows(c, Xd.shape[1])
+    for s in range(0, n, step):
+        e = min(s + step, n)
+        flat = cols[s:e].reshape(-1)
+        dots = np.einsum("id,icd->ic", Xh[s:e], Xh[flat].reshape(e - s, c, Xd.shape[1]))
+        dots = dots.astype(np.float16).astype(np.float32)
+        out[s:e] = np.maximum(sq[s:e, None] + sq[flat].reshape(e - s, c) - np.float32(2.0) * dots, np.float32(0))
+    return out
 
 
 def reverse_candidates(indices: np.ndarray) -> np.ndarray:
@@ -123,10 +139,14 @@ def build(X, k=15, n_iters=20, max_candidates=None, delta=0.015, random_state=No
             nc = nc.reshape(len(active), mc_new * j_nn)
             if use_rev:
                 nc = np.concatenate([nc, reverse_candidates(indices)[active]], axis=1)
-            flat = nc.reshape(-1)
-            dots = np.einsum("id,icd->ic", X[active], X[flat].reshape(len(active), nc.shape[1], d))
-            new_d = np.maximum(sq[active, None] + sq[flat].reshape(nc.shape) - np.float32(2.0) * dots,
-                               np.float32(0))
+            new_d = np.empty(nc.shape, dtype=np.float32)
+            step = _chunk_rows(nc.shape[1], d)
+            for s in range(0, len(active), step):
+                e = min(s + step, len(active))
+                flat = nc[s:e].reshape(-1)
+                dots = np.einsum("id,icd->ic", X[active[s:e]], X[flat].reshape(e - s, nc.shape[1], d))
+                new_d[s:e] = np.maximum(sq[active[s:e], None] + sq[flat].reshape(e - s, nc.shape[1])
+                                        - np.float32(2.0) * dots, np.float32(0))
             ac = np.concatenate([indices[active], nc], axis=1)
             ad = np.concatenate([dists[active], new_d], axis=1)
             ad = np.where(ac == active[:, None], _BIG, ad)

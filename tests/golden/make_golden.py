@@ -33,13 +33,15 @@ warnings.simplefilter("ignore", RuntimeWarning)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("MLX_VIS_REFERENCE", "/root/reference")
+REF = os.environ.get("MLX_VIS_REFERENCE")
 
 sys.path.insert(0, os.path.join(REPO, "oracle", "mlx_shim"))
 sys.path.insert(0, REPO)
 
 
 def _load_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "mlx_vis")):
+        raise SystemExit("set MLX_VIS_REFERENCE to a checkout of hanxiao/mlx-vis (the directory holding mlx_vis/)")
     for name, sub in [("mlx_vis", "mlx_vis"), ("mlx_vis._umap", "mlx_vis/_umap"),
                       ("mlx_vis._nndescent", "mlx_vis/_nndescent")]:
         mod = types.ModuleType(name)

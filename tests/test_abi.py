@@ -60,8 +60,11 @@ def test_workspace_queries_and_argument_errors(lib):
     with pytest.raises(_lib.UmapB200Error, match="<= 128"):
         _lib.query("umapb_knn_brute_workspace", 1000, 4, 100, 40)
     assert _lib.query("umapb_fuzzy_workspace", 1000, 15) > 1000 * 15 * 8
-    with pytest.raises(_lib.UmapB200Error):
-        _lib.query("umapb_spectral_workspace", 100, 7, 1000, 100)
+    assert _lib.query("umapb_spectral_workspace", 100, 7, 1000, 100) > 0  # n_components up to 32
+    with pytest.raises(_lib.UmapB200Error, match="dim <= 32"):
+        _lib.query("umapb_spectral_workspace", 100, 33, 1000, 100)
+    with pytest.raises(_lib.UmapB200Error, match="dim <= 32"):
+        _lib.query("umapb_layout_workspace", 100, 33, 1000)
     assert _lib.load().umapb_abi_version() == 1
 
 

@@ -104,12 +104,34 @@ def test_spectral_paths_agree_for_every_dim(golden, monkeypatch, dim):
     assert np.abs(out["1"] - out["0"]).max() < 1e-3
 
 
-def _layout(fz, n=2000, n_epochs=200):
+@pytest.mark.parametrize("dim", [5, 8, 32])
+def test_wide_spectral_matches_fp64_oracle(golden, dim):
+    """n_components above 4: one launch per power iteration, one warp per row, the
+    Gram matrix factored by the last block; against the FP64 oracle of umap.py:298-348."""
+    from mlx_vis_b200 import _lib
+
+    fz = golden("fuzzy_gauss")
+    n = 2000
+    rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
+    ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
+    V0 = np.random.RandomState(dim).normal(size=(n, dim + 1)).astype(np.float32)
+    noise = np.random.RandomState(42).normal(scale=0.0001, size=(n, dim)).astype(np.float32)
+    Y = _lib.spectral(rows, cols, vals, ne, n, dim, cuda(V0), cuda(noise), n_iter=100, check=True).cpu().numpy()
+    V = ospec.power_iteration(fz["rows"], fz["cols"], fz["vals"], n, V0, dtype=np.float64)
+    Y64 = ospec.rescale(V[:, 1:].astype(np.float32), 42)
+    assert Y.shape == (n, dim)
+    # columns whose eigenvalues nearly coincide converge slowly in both; compare the
+    # well-separated leading columns tightly and all columns on the whole
+    assert np.abs(Y[:, :2] - Y64[:, :2]).max() < 1e-3
+    assert np.median(np.abs(Y - Y64)) < 1e-3
+
+
+def _layout(fz, n=2000, n_epochs=200, dim=2):
     from mlx_vis_b200 import _lib
 
     rows, cols, vals = cuda(fz["rows"]), cuda(fz["cols"]), cuda(fz["vals"])
     ne = torch.tensor([rows.numel()], dtype=torch.int64, device="cuda")
-    return _lib.Layout(rows, cols, vals, ne, n, 2, n_epochs)
+    return _lib.Layout(rows, cols, vals, ne, n, dim, n_epochs)
 
 
 def test_schedule_active_counts_match_reference(golden, manifest):
@@ -150,6 +172,29 @@ def test_injected_epochs_match_reference(golden, manifest):
     ref = opt["Y_ep3"]
     # after a second epoch the steep short-range forces amplify rounding; stay close
     assert np.median(np.abs(got - ref)) < 1e-5 and np.abs(got - ref).max() < 1e-2
+
+
+@pytest.mark.parametrize("dim", [5, 8, 32])
+def test_wide_injected_epoch_matches_oracle(golden, manifest, dim):
+    """One epoch at n_components above 4 (one warp per edge) with injected tails,
+    against the FP32 oracle of umap.py:359-387."""
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    lay = _layout(fz, dim=dim)
+    rng = np.random.default_rng(dim)
+    Y0 = rng.uniform(0, 10, size=(2000, dim)).astype(np.float32)
+    Y = cuda(Y0.copy())
+    sets = olay.active_sets(fz["vals"], 200)
+    e = next(t for t in range(200) if len(sets[t]) > 0)
+    lay.epochs(Y, 0, e, m["a"], m["b"], 1.0, 5, 0)
+    A = len(sets[e])
+    neg = rng.integers(0, 2000, 5 * A).astype(np.int32)
+    lay.epoch_injected(Y, e, m["a"], m["b"], 1.0, 5, cuda(neg))
+    got = Y.cpu().numpy()
+    Yo = olay.sgd_epoch(Y0, fz["rows"][sets[e]], fz["cols"][sets[e]], np.resize(fz["rows"][sets[e]], 5 * A),
+                        neg.astype(np.int64), 1.0 * (1 - e / 200), m["a"], m["b"])
+    assert np.abs(got - Y0).max() > 1e-3  # the epoch moved the points
+    assert np.abs(got - Yo).max() <= 1e-4, np.abs(got - Yo).max()
 
 
 def test_injected_negative_count_is_checked(golden, manifest):

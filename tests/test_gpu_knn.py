@@ -107,6 +107,26 @@ def test_brute_argument_errors():
         _lib.knn_brute(torch.zeros((500, 4), device="cuda"), 120, extra=16)
 
 
+def test_compute_knn_nndescent_branch(golden):
+    """compute_knn(method="nndescent") (_knn.py:35-45): seed 42 when random_state is
+    None, the NNDescent graph unchanged, squared distances for return_euclidean=False;
+    the graph agrees with the reference's NNDescent on the same data and seed."""
+    from mlx_vis_b200 import NNDescent, datasets
+    from mlx_vis_b200._knn import compute_knn
+
+    Xn = datasets.gaussian_mixture(3000, 32, seed=2)
+    idx, dist = compute_knn(Xn, 15, method="nndescent")
+    assert idx.dtype == np.int32 and dist.dtype == np.float32 and idx.shape == (3000, 15)
+    ref_i, ref_d = NNDescent(k=15, random_state=42).build(Xn)
+    assert np.array_equal(idx, ref_i) and np.array_equal(dist, ref_d)
+    idx_sq, d2 = compute_knn(Xn, 15, method="nndescent", return_euclidean=False)
+    assert np.array_equal(idx_sq, idx) and np.array_equal(d2, dist ** 2)
+    idx7, _ = compute_knn(Xn, 15, method="nndescent", random_state=7)
+    assert not np.array_equal(idx7, idx)  # the seed reaches NNDescent
+    g = golden("nnd_gauss")
+    assert np.mean(idx == g["idx_it20"]) > 0.99
+
+
 def test_compute_knn_plug_point(gauss2000, golden):
     from mlx_vis_b200._knn import compute_knn
 
@@ -134,24 +154,76 @@ def test_brute_tile_paths_ragged(n, d, k, tile_path):
     assert_exact_knn(X, idx, dist, k)
 
 
+def exact_knn_f64_cuda(X: np.ndarray, k: int, cand: int = 48, chunk: int = 2048):
+    """Exact kNN of every row in float64 on the GPU (test-side checker, torch
+    float64): expanded-form distances pick the best `cand` candidates, whose
+    distances are then recomputed as sum (x_i - x_j)^2; (distance, index) order."""
+    Xd = torch.from_numpy(X).cuda().double()
+    n = Xd.shape[0]
+    sq = (Xd * Xd).sum(1)
+    out_i = torch.empty((n, k), dtype=torch.int64, device="cuda")
+    out_d = torch.empty((n, k), dtype=torch.float64, device="cuda")
+    for s in range(0, n, chunk):
+        e = min(s + chunk, n)
+        D = sq[s:e, None] + sq[None, :] - 2.0 * (Xd[s:e] @ Xd.T)
+        D[torch.arange(e - s, device="cuda"), torch.arange(s, e, device="cuda")] = float("inf")
+        c = torch.topk(D, cand, dim=1, largest=False).indices
+        d2 = ((Xd[c] - Xd[s:e, None, :]) ** 2).sum(-1)
+        # order by (distance, index): index breaks exact ties
+        key = torch.argsort(c, dim=1, stable=True)
+        c, d2 = torch.gather(c, 1, key), torch.gather(d2, 1, key)
+        o = torch.argsort(d2, dim=1, stable=True)[:, :k]
+        out_i[s:e] = torch.gather(c, 1, o)
+        out_d[s:e] = torch.gather(d2, 1, o)
+    return out_i.cpu().numpy(), out_d.cpu().numpy()
+
+
 def test_brute_tile_paths_agree_at_scale(tile_path):
-    """20000 x 784 (several row blocks per unit, candidate slots > 1): sampled
-    rows against the float64 exact kNN."""
+    """The 20000 x 784 exact-kNN workload (several row blocks per unit, candidate
+    slots > 1): EVERY row against the float64 exact kNN, ties within 1e-6 relative
+    distance allowed to swap."""
     from mlx_vis_b200 import datasets
 
     X = datasets.prototype_mixture(20000, 784, seed=0)
     idx, dist = run_knn(X, 15)
-    rows = np.random.default_rng(1).choice(X.shape[0], 300, replace=False)
-    Xd = X.astype(np.float64)
-    sq = np.sum(Xd * Xd, axis=1)
-    D = sq[rows, None] + sq[None, :] - 2.0 * (Xd[rows] @ Xd.T)
-    D[np.arange(len(rows)), rows] = np.inf
-    cand = np.argpartition(D, 40, axis=1)[:, :40]  # exact top-15 lies among them
-    for i, r in enumerate(rows):
-        c = cand[i]
-        d2 = np.sum((Xd[c] - Xd[r]) ** 2, axis=1)
-        o = np.lexsort((c, d2))[:15]
-        want = d2[o]
-        ours = np.sum((Xd[idx[r]] - Xd[r]) ** 2, axis=1)
-        assert np.all(np.abs(ours - want) <= TIE * np.maximum(want, 1e-12) + 1e-12), r
-        np.testing.assert_allclose(dist[r], np.sqrt(want), rtol=2e-6, atol=1e-6)
+    want_i, want_d2 = exact_knn_f64_cuda(X, 15)
+    Xt = torch.from_numpy(X).cuda().double()
+    ours_d2 = ((Xt[torch.from_numpy(idx).cuda().long()] - Xt[:, None, :]) ** 2).sum(-1).cpu().numpy()
+    assert np.all(idx != np.arange(len(X))[:, None])
+    assert all(len(set(r)) == 15 for r in idx)
+    # the sorted distance profile equals the exact one up to ties
+    assert np.all(np.abs(ours_d2 - want_d2) <= TIE * np.maximum(want_d2, 1e-12) + 1e-12)
+    np.testing.assert_allclose(dist, np.sqrt(want_d2), rtol=2e-6, atol=1e-6)
+    # indices equal the exact ones wherever the distance is not tied
+    agree = np.mean(idx == want_i)
+    assert agree > 0.999, agree
+
+
+@pytest.mark.parametrize("n,d,parts", [(3000, 64, 3), (20000, 784, 2), (1000, 130, 7)])
+def test_brute_rows_blocks_reassemble_the_full_result(n, d, parts, tile_path):
+    """umapb_knn_brute_rows on the blocks of a row split (the per-rank work of the
+    sharded kNN) gives the rows of umapb_knn_brute: same indices, same distances."""
+    from mlx_vis_b200 import _lib
+    from mlx_vis_b200._distributed import knn_brute_sharded, row_blocks
+
+    X = np.random.default_rng(n + d).normal(size=(n, d)).astype(np.float32)
+    Xd = torch.from_numpy(X).cuda()
+    ref_i, ref_d = _lib.knn_brute(Xd, 15)
+    got = [_lib.knn_brute_rows(Xd, 15, b, c) for b, c in row_blocks(n, parts)]
+    idx = torch.cat([g[0] for g in got])
+    dst = torch.cat([g[1] for g in got])
+    assert torch.equal(idx, ref_i)
+    torch.testing.assert_close(dst, ref_d, rtol=1e-6, atol=1e-6)
+    # one process, no group: the sharded entry runs the whole range
+    i1, d1 = knn_brute_sharded(Xd, 15)
+    assert torch.equal(i1, ref_i)
+
+
+def test_brute_rows_argument_errors():
+    from mlx_vis_b200 import _lib
+
+    X = torch.zeros((100, 4), device="cuda")
+    with pytest.raises(_lib.UmapB200Error, match="query rows"):
+        _lib.knn_brute_rows(X, 5, 90, 20)
+    with pytest.raises(_lib.UmapB200Error, match="query rows"):
+        _lib.knn_brute_rows(X, 5, -1, 2)

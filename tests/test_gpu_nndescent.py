@@ -235,3 +235,48 @@ def test_join_and_row_kernel_builds_agree(name, gen, monkeypatch):
     np.testing.assert_allclose(out["1"][2], out["0"][2], rtol=0.02, atol=20)
     same = out["1"][0] == out["0"][0]
     np.testing.assert_allclose(out["1"][1][same], out["0"][1][same], rtol=1e-3, atol=1e-3)
+
+
+@pytest.mark.parametrize("k,gen", [(40, ("gaussian_mixture", 3000, 32, 2)), (91, ("gaussian_mixture", 2500, 16, 5)),
+                                   (50, ("prototype_mixture", 2000, 784, 3))])
+def test_nndescent_large_k_tracks_oracle(k, gen):
+    """k above 32 (one block per row, every candidate distance in the row kernel;
+    nnd_wide.cu): the same random start and iteration rules as the oracle, so the
+    per-iteration update counts and the final graph follow it; the reference itself
+    is calibrated at k = 91 (nndescent.py:85-88)."""
+    from mlx_vis_b200 import NNDescent, datasets
+
+    X = getattr(datasets, gen[0])(gen[1], gen[2], seed=gen[3])
+    nn = NNDescent(k=k, random_state=42)
+    idx, dist = nn.build(X)
+    (oidx, odist), log = onnd.build(X, k=k, random_state=42, history=True)
+    ours = np.array([h["changed"] for h in nn.history_])
+    ref = np.array([l["changed"] for l in log])
+    assert len(ours) == len(ref), (ours, ref)
+    np.testing.assert_allclose(ours, ref, rtol=0.02, atol=20)
+    overlap = np.mean([len(set(a) & set(b)) / k for a, b in zip(idx, oidx)])
+    assert overlap > 0.99, overlap
+    assert np.all(idx != np.arange(len(X))[:, None])
+    assert all(len(set(r)) == k for r in idx)
+    assert np.all(np.diff(dist, axis=1) >= 0)
+    ri, _ = oknn.knn_exact_f64(X, k)
+    assert abs(recall(idx, ri) - recall(oidx, ri)) < 0.01
+
+
+def test_umap_with_fifty_neighbours(gauss2000):
+    """UMAP(n_neighbors=50, knn_method="nndescent") runs end to end (the reference
+    has no limit on k)."""
+    from sklearn.manifold import trustworthiness
+
+    from mlx_vis_b200 import UMAP
+
+    Y = UMAP(n_neighbors=50, n_epochs=100, knn_method="nndescent", random_state=0).fit_transform(gauss2000)
+    assert Y.shape == (2000, 2) and np.isfinite(Y).all()
+    assert trustworthiness(gauss2000, Y, n_neighbors=15) > 0.93
+
+
+def test_nndescent_k_above_the_envelope_is_rejected():
+    from mlx_vis_b200 import NNDescent
+
+    with pytest.raises(ValueError, match="k <= 100"):
+        NNDescent(k=101).build(np.zeros((200, 4), dtype=np.float32))

@@ -53,7 +53,7 @@ def test_n_epochs_default_is_written_back():
     assert u.n_epochs == 500
 
 
-@pytest.mark.parametrize("n_components", [1, 3])
+@pytest.mark.parametrize("n_components", [1, 3, 5, 8, 32])
 def test_other_output_dims(n_components):
     from mlx_vis_b200 import UMAP
     from mlx_vis_b200.datasets import gaussian_mixture
@@ -91,3 +91,57 @@ def test_nndescent_waits_for_the_upload_after_its_random_start(gauss2000):
     idx_a, dist_a = NNDescent(k=15, random_state=7).build_device(Xd, x_ready=ready)
     idx_b, dist_b = NNDescent(k=15, random_state=7).build_device(torch.from_numpy(gauss2000).cuda())
     assert torch.equal(idx_a, idx_b) and torch.equal(dist_a, dist_b)
+
+
+def test_wide_embedding_keeps_neighbourhoods(gauss2000):
+    """n_components above 4 (warp-per-row spectral init, warp-per-edge epochs): the
+    embedding of the 10-cluster mixture stays trustworthy like the 2-d one."""
+    from mlx_vis_b200 import UMAP
+
+    Y = UMAP(n_components=8, n_epochs=200, knn_method="brute", random_state=0).fit_transform(gauss2000)
+    assert Y.shape == (2000, 8) and np.isfinite(Y).all()
+    assert trustworthiness(gauss2000, Y, n_neighbors=15) > 0.95
+
+
+def test_n_components_outside_the_envelope_is_rejected():
+    from mlx_vis_b200 import UMAP
+
+    with pytest.raises(ValueError, match="n_components"):
+        UMAP(n_components=33).fit_transform(np.zeros((10, 3), dtype=np.float32))
+
+
+def test_spectral_failure_falls_back_to_the_random_start(gauss2000):
+    """The reference falls back to a random start when its spectral init fails
+    (umap.py:354-357).  Here the failure is the power iteration's bounded grid
+    barrier giving up: a 1 ns limit makes every wait expire (no GPU fault, the
+    kernel returns), the device swaps in normal((n, c), seed) * 0.01, and the fit
+    reports init_used_ == "random"."""
+    import torch
+
+    from mlx_vis_b200 import UMAP, _lib
+
+    n = 20000
+    X = np.concatenate([gauss2000] * 10)[:n] + np.random.default_rng(0).normal(scale=0.01, size=(n, 64)).astype(
+        np.float32)
+    Xd = torch.from_numpy(X.astype(np.float32)).cuda()
+    idx, dist = _lib.knn_brute(Xd, 15)
+    rows, cols, vals, ne = _lib.fuzzy(idx, dist, 200)
+    V0 = _lib.normal((n, 3), 1, Xd.device)
+    noise = _lib.normal((n, 2), 2, Xd.device) * 1e-4
+    ok, ws_ok = _lib.spectral(rows, cols, vals, ne, n, 2, V0, noise, fallback_seed=9, return_workspace=True)
+    assert _lib.status_word(ws_ok) == 0
+    try:
+        _lib.set_wait_limit_ns(1)
+        Y, ws = _lib.spectral(rows, cols, vals, ne, n, 2, V0, noise, fallback_seed=9, return_workspace=True)
+        assert _lib.status_word(ws) != 0
+        want = _lib.normal((n, 2), 9, Xd.device) * 0.01
+        assert torch.equal(Y, want)
+        assert not torch.equal(ok, want)
+        u = UMAP(n_epochs=20, knn_method="brute", random_state=4)
+        Yu = u.fit_transform(Xd)
+        assert u.init_used_ == "random" and np.isfinite(Yu).all()
+    finally:
+        _lib.set_wait_limit_ns(0)
+    u = UMAP(n_epochs=20, knn_method="brute", random_state=4)
+    u.fit_transform(Xd)
+    assert u.init_used_ == "spectral"

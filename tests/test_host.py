@@ -109,3 +109,20 @@ def test_mt19937_restatement_matches_numpy(n, k, d, seed):
     # the uint32 state buffer of umapb_nnd_random_start round-trips
     back = words_state(state_words(st_h))
     assert np.array_equal(back[1], st_h[1]) and back[2:] == st_h[2:]
+
+
+def test_fit_sampler_scales_full_size_samples():
+    """oracle.pipeline.FitSampler (the CPU baseline): every stage runs on the full
+    input and each estimate is a positive, finite number of seconds."""
+    from mlx_vis_b200.datasets import prototype_mixture
+    from oracle import nndescent as onnd
+    from oracle.pipeline import FitSampler
+
+    X = prototype_mixture(1200, 64, seed=2)
+    (idx, _), log = onnd.build(X, k=10, random_state=0, history=True)
+    fs = FitSampler(X, idx, [h["changed"] for h in log], n_epochs=50, block=200, epochs_per_step=2)
+    r = fs.step()
+    assert set(r) == {"knn", "fuzzy", "init", "layout", "fit"}
+    assert all(np.isfinite(v) and v > 0 for v in r.values())
+    assert abs(r["fit"] - (r["knn"] + r["fuzzy"] + r["init"] + r["layout"])) < 1e-9
+    assert fs.updates_total > 0 and "1200 x 64" in fs.describe()

@@ -111,3 +111,30 @@ def test_nndescent_oracle_tracks_reference(name, gen, golden):
         ref = g[f"updates_it{t}"]
         assert len(ours) == len(ref)
         np.testing.assert_allclose(ours, ref, rtol=0.01, atol=10)
+
+
+def test_pca_oracle_matches_reference(golden, manifest):
+    """The float64 PCA restatement against the reference's own X_for_knn
+    (umap.py:92-113 on the NumPy mlx shim), per column up to sign."""
+    from mlx_vis_b200.datasets import prototype_mixture
+    from oracle import pca as opca
+
+
+    X = prototype_mixture(1000, 784, seed=4)
+    assert _sha(X) == manifest["pca_proto"]["sha"]
+    ref = golden("pca_proto")["X_pca"].astype(np.float64)
+    got, _, _ = opca.pca(X, 20)
+    assert np.abs(opca.align_signs(ref, got) - ref).max() < 1e-3 * np.abs(ref).max()
+
+
+def test_c3_fixture_input_is_the_benchmark_workload(golden, manifest):
+    """The 70,000 x 784 fixture was made from the benchmark's own generator."""
+    from mlx_vis_b200.datasets import prototype_mixture
+
+
+    m = manifest["c3_70k"]
+    X = prototype_mixture(70000, 784, seed=0)
+    assert _sha(X) == m["sha"]
+    g = golden("c3_70k")
+    assert g["idx"].shape == (70000, 15) and g["exact_idx"].shape == (2000, 15)
+    assert len(g["updates"]) == 9 and m["n_edges"] > 0

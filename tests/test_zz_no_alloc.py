@@ -58,6 +58,20 @@ def test_noalloc_squared_distances_match():
         torch.testing.assert_close(d2, ref_d2, rtol=1e-6, atol=1e-6)
 
 
+def test_noalloc_serves_long_candidate_lists():
+    """k + extra = 128 on 1000 rows: the candidate merge needs more than 48 KB of
+    shared memory per block, which the allocation-free entry point raises per
+    device like the workspace entry point."""
+    from mlx_vis_b200 import _lib
+
+    X = torch.from_numpy(np.random.default_rng(2).normal(size=(1000, 24)).astype(np.float32)).cuda()
+    ref_idx, ref_dist = _lib.knn_brute(X, 112, extra=16)
+    for _ in range(2):
+        idx, dist, status = knn_noalloc(X, 112, extra=16)
+        assert status == 0 and torch.equal(idx, ref_idx)
+        torch.testing.assert_close(dist, ref_dist, rtol=1e-6, atol=1e-6)
+
+
 def test_noalloc_rejects_requests_beyond_its_scratch():
     from mlx_vis_b200 import _lib
 
