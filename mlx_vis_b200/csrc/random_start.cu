@@ -261,41 +261,48 @@ struct Scalars {
 
 // raw[n] = x_n of the MT sequence: x_0..x_623 is the incoming key (generation 0)
 // and x_n = x_{n-227} ^ mix(x_{n-624}, x_{n-623}) for n >= 624, so raw[624 g + i] is
-// word i of generation g.  Words [n, n + 227) depend only on earlier blocks of 227:
-// thread t computes word base + t of every block, keeps x_{n-227} (its own previous
-// word) in a register and loads x_{n-624}, x_{n-623} (two or more blocks old) one
-// block ahead from a shared ring, so a block costs one barrier.
-__global__ void __launch_bounds__(kPar) stream_kernel(const uint32_t* __restrict__ state, int64_t total,
-                                                      uint32_t* __restrict__ raw) {
-  __shared__ uint32_t ring[1024];
+// word i of generation g.  mix is linear over GF(2) and x_{n-227}, x_{n-454} unfold
+// by the same recurrence, so for n >= 1078
+//   x_n = x_{n-681} ^ mix(x_{n-1078}, x_{n-1077}) ^ mix(x_{n-851}, x_{n-850})
+//                   ^ mix(x_{n-624}, x_{n-623}),
+// whose nearest operand is 623 words back: a block of 623 words depends only on
+// earlier blocks, so one barrier covers 623 words (the plain recurrence allows 227).
+// Words 624..1077 use the plain recurrence in two blocks of 227.  A block writes
+// ring slots n mod 2048 that none of its reads touch (those lie 456..1700 slots
+// away), so every block costs one barrier.
+constexpr int kStreamThreads = 640;
+constexpr int kWide = 623;
+constexpr int kRing = 2048;
+
+__global__ void __launch_bounds__(kStreamThreads) stream_kernel(const uint32_t* __restrict__ state, int64_t total,
+                                                                uint32_t* __restrict__ raw) {
+  __shared__ uint32_t ring[kRing];
+  constexpr int R = kRing - 1;
   const int t = threadIdx.x;
-  for (int i = t; i < kN; i += kPar) {
+  for (int i = t; i < kN; i += kStreamThreads) {
     const uint32_t v = state[i];
     ring[i] = v;
     raw[i] = v;
   }
   __syncthreads();
-  const bool act = t < kHalf;
-  // block 0 (n = 624 + t) reads x_t, x_{t+1}; block 1 reads x_{227+t}, x_{228+t}
-  uint32_t a0 = act ? ring[t] : 0u, b0 = act ? ring[t + 1] : 0u;
-  uint32_t a1 = act ? ring[kHalf + t] : 0u, b1 = act ? ring[kHalf + t + 1] : 0u;
-  uint32_t prev = act ? ring[kM + t] : 0u;  // x_{n-227} for block 0
-  for (int64_t base = kN; base < total; base += kHalf) {
+  for (int64_t base = kN; base < 1078 && base < total; base += kHalf) {
     const int64_t n = base + t;
-    if (act) {
-      const uint32_t x = prev ^ mix(a0, b0);
-      prev = x;
-      ring[n & 1023] = x;
-      if (n < total) raw[n] = x;
+    if (t < kHalf && n < total) {
+      const uint32_t x = ring[(n - kHalf) & R] ^ mix(ring[(n - kN) & R], ring[(n - kN + 1) & R]);
+      ring[n & R] = x;
+      raw[n] = x;
     }
     __syncthreads();
-    // operands of the block after next (n + 454): x_{n-170}, x_{n-169}, both written by now
-    a0 = a1;
-    b0 = b1;
-    if (act) {
-      a1 = ring[(n - 170) & 1023];
-      b1 = ring[(n - 169) & 1023];
+  }
+  for (int64_t base = 1078; base < total; base += kWide) {
+    const int64_t n = base + t;
+    if (t < kWide && n < total) {
+      const uint32_t x = ring[(n - 681) & R] ^ mix(ring[(n - 1078) & R], ring[(n - 1077) & R]) ^
+                         mix(ring[(n - 851) & R], ring[(n - 850) & R]) ^ mix(ring[(n - 624) & R], ring[(n - 623) & R]);
+      ring[n & R] = x;
+      raw[n] = x;
     }
+    __syncthreads();
   }
 }
 
@@ -506,7 +513,7 @@ static int run_parallel(const Plan& p, uint32_t* state, int64_t count, int k, ui
   UMAPB_CUDA_TRY(cudaMemcpyAsync(p.backup, state, (kN + 4) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
                  "random draws: state copy");
   int launches = 3;
-  stream_kernel<<<1, kPar, 0, stream>>>(state, (p.n_gen + 1) * kN, p.raw);
+  stream_kernel<<<1, kStreamThreads, 0, stream>>>(state, (p.n_gen + 1) * kN, p.raw);
   if (count > 0 && rng == 0) {
     const int64_t want = (count + 255) / 256;
     const_ints_kernel<<<(unsigned)(want < 4096 ? want : 4096), 256, 0, stream>>>(count, k, idx);
