@@ -11,9 +11,9 @@ offline), NNDescent k=15 with the reference's defaults (n_iters 20, delta
   fit_s   seconds per fit (the other half of the metric)
   e2e     the same metric through UMAP.fit_transform on a pinned host tensor,
           host->device input and device->host embedding copies inside the timing
-  roofline  the layout epoch (one fused sgd_epoch_kernel launch per epoch), the
-          largest kernel share of a fit: 112 algorithmic bytes per active edge
-          over the layout stage's CUDA-event time divided by the epochs
+  roofline  the layout epoch (sgd_epoch_kernel + apply_kernel), the largest
+          kernel share of a fit: 112 algorithmic bytes per active edge over the
+          layout stage's CUDA-event time divided by the epochs
   roofline_nndescent  one NNDescent iteration (join + row kernel), CUDA events
           around each launch in the timed fits, against two byte counts: every
           reference candidate row read once, and the rows the blocked join reads

@@ -352,11 +352,21 @@ def split3(S: torch.Tensor, mu=None, transpose: bool = False, kp: int | None = N
     return out, kp
 
 
-def gemm_split3(A3: torch.Tensor, B3: torch.Tensor, kp: int, ksplit: int = 1, scale: float = 1.0,
+SPLIT_SLICE_K = 1024  # K values per accumulator slice when ksplit is chosen automatically
+
+
+def gemm_split3(A3: torch.Tensor, B3: torch.Tensor, kp: int, ksplit: int | None = None, scale: float = 1.0,
                 status: torch.Tensor | None = None) -> torch.Tensor:
-    """C = A B^T (M x N, float32) from split operands (FP32-level products on tcgen05)."""
+    """C = A B^T (M x N, float32) from split operands (FP32-level products on tcgen05).
+
+    The tensor cores add the products of one accumulator in FP32; over a long K
+    (a covariance over tens of thousands of rows, all products of a diagonal entry
+    positive) that rounding grows with K, so by default the K range is cut into
+    slices of at most 1024 values whose partial results are summed in FP64."""
     M, N = A3.shape[0], B3.shape[0]
     dev = A3.device
+    if ksplit is None:
+        ksplit = max(1, min(4096, -(-int(kp) // SPLIT_SLICE_K)))
     st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
     C = torch.empty((ksplit, M, N), dtype=torch.float32, device=dev)
     call("umapb_gemm_split3", ptr(A3), ptr(B3), M, N, int(kp), int(ksplit), ptr(C), N, ptr(st), stream_handle())

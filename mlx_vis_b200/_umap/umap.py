@@ -178,9 +178,8 @@ class UMAP:
         n, d = Xd.shape
         mean = _lib.colmean(Xd)
         XT3, kpn = _lib.split3(Xd, mu=mean, transpose=True)  # operand rows = features, K = samples
-        tiles = ((d + 127) // 128) ** 2
-        ksplit = max(1, min(16, 148 // max(tiles, 1)))
-        cov = _lib.gemm_split3(XT3, XT3, kpn, ksplit=ksplit, scale=1.0 / max(n - 1, 1))
+        # K = n rows, cut into slices of at most 1024 rows summed in FP64
+        cov = _lib.gemm_split3(XT3, XT3, kpn, scale=1.0 / max(n - 1, 1))
         del XT3
         evals, evecs = np.linalg.eigh(to_host(cov).astype(np.float64))
         proj = np.ascontiguousarray(evecs[:, -self.pca_dim:][:, ::-1], dtype=np.float32)

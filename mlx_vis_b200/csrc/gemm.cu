@@ -292,7 +292,7 @@ extern "C" int umapb_gemm_split3(const void* A3, const void* B3, int32_t M, int3
                 "gemm_split3: need M, N >= 1 and kp a positive multiple of 64");
   UMAPB_REQUIRE((int64_t)kp * 3 < ((int64_t)1 << 31), "gemm_split3: kp too large");
   UMAPB_REQUIRE(ldc >= N, "gemm_split3: ldc must be >= N");
-  UMAPB_REQUIRE(ksplit >= 1 && ksplit <= 64, "gemm_split3: ksplit must be in [1, 64]");
+  UMAPB_REQUIRE(ksplit >= 1 && ksplit <= 4096, "gemm_split3: ksplit must be in [1, 4096]");
   static bool attr[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);

@@ -120,105 +120,6 @@ __device__ __forceinline__ void atomic_add_row(float* __restrict__ dY, int i, co
   }
 }
 
-// ---- fused epochs: the apply step folded into the next epoch -----------------
-// Three rotating buffers X_0, X_1, X_2 of FP floats per row hold [y | d]: y the
-// coordinates at the start of the previous epoch and d the summed moves of that
-// epoch, so the coordinates at the start of epoch t are Y_t = y + d of X_{t mod 3}
-// (the same float32 addition as the separate apply step).  Epoch t reads only
-// X_t; it adds its moves into X_{t+1}.d, writes X_{t+1}.y = Y_t for every row, and
-// clears X_{t+2}.d (last read in epoch t-1) for the epoch after.  No word is both
-// read and written within an epoch, so one launch per epoch keeps the reference's
-// synchronous scatter-add semantics.
-template <int DIM>
-struct Fused {
-  static constexpr int FP = DIM == 1 ? 2 : (DIM == 2 ? 4 : 8);  // floats per row
-  static constexpr int DOFF = DIM == 1 ? 1 : (DIM == 2 ? 2 : 4); // offset of d
-};
-
-template <int DIM, bool FUSED>
-__device__ __forceinline__ void load_y(const float* __restrict__ Y, int i, float (&v)[DIM]) {
-  if constexpr (!FUSED) {
-    load_row<DIM>(Y, i, v);
-  } else if constexpr (DIM == 1) {
-    const float2 t = __ldg(reinterpret_cast<const float2*>(Y) + i);
-    v[0] = __fadd_rn(t.x, t.y);
-  } else if constexpr (DIM == 2) {
-    const float4 t = __ldg(reinterpret_cast<const float4*>(Y) + i);
-    v[0] = __fadd_rn(t.x, t.z);
-    v[1] = __fadd_rn(t.y, t.w);
-  } else {
-    const float4 a = __ldg(reinterpret_cast<const float4*>(Y) + 2 * (int64_t)i);
-    const float4 b = __ldg(reinterpret_cast<const float4*>(Y) + 2 * (int64_t)i + 1);
-    v[0] = __fadd_rn(a.x, b.x);
-    v[1] = __fadd_rn(a.y, b.y);
-    v[2] = __fadd_rn(a.z, b.z);
-    if constexpr (DIM == 4) v[3] = __fadd_rn(a.w, b.w);
-  }
-}
-
-template <int DIM, bool FUSED>
-__device__ __forceinline__ void add_move(float* __restrict__ dY, int i, const float (&v)[DIM]) {
-  if constexpr (!FUSED) {
-    atomic_add_row<DIM>(dY, i, v);
-  } else {
-    float* d = dY + (int64_t)i * Fused<DIM>::FP + Fused<DIM>::DOFF;
-    if constexpr (DIM == 1) {
-      atomicAdd(d, v[0]);
-    } else if constexpr (DIM == 2) {
-      atomicAdd(reinterpret_cast<float2*>(d), make_float2(v[0], v[1]));
-    } else if constexpr (DIM == 3) {
-      atomicAdd(reinterpret_cast<float2*>(d), make_float2(v[0], v[1]));
-      atomicAdd(d + 2, v[2]);
-    } else {
-      atomicAdd(reinterpret_cast<float4*>(d), make_float4(v[0], v[1], v[2], v[3]));
-    }
-  }
-}
-
-// X_{t+1}.y = y + d of X_t and X_{t+2}.d = 0 for rows [r0, n) with stride
-template <int DIM>
-__device__ __forceinline__ void fold_rows(const float* __restrict__ Xc, float* __restrict__ Xn,
-                                          float* __restrict__ Xz, int n, int64_t r0, int64_t stride) {
-  constexpr int FP = Fused<DIM>::FP, DO = Fused<DIM>::DOFF;
-  for (int64_t r = r0; r < n; r += stride) {
-    float v[DIM];
-    load_y<DIM, true>(Xc, (int)r, v);
-    if constexpr (DIM == 1) {
-      Xn[r * FP] = v[0];
-      Xz[r * FP + DO] = 0.f;
-    } else if constexpr (DIM == 2) {
-      *reinterpret_cast<float2*>(Xn + r * FP) = make_float2(v[0], v[1]);
-      *reinterpret_cast<float2*>(Xz + r * FP + DO) = make_float2(0.f, 0.f);
-    } else {
-      *reinterpret_cast<float4*>(Xn + r * FP) = make_float4(v[0], v[1], v[2], DIM == 4 ? v[3] : 0.f);
-      *reinterpret_cast<float4*>(Xz + r * FP + DO) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-  }
-}
-
-// X_0 = [Y | 0], X_1.d = 0 (before the first fused epoch)
-template <int DIM>
-__global__ void fused_init_kernel(const float* __restrict__ Y, float* __restrict__ X0, float* __restrict__ X1, int n) {
-  constexpr int FP = Fused<DIM>::FP, DO = Fused<DIM>::DOFF;
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  for (int c = 0; c < FP; ++c) {
-    X0[r * FP + c] = c < DIM ? Y[r * DIM + c] : 0.f;
-    if (c >= DO) X1[r * FP + c] = 0.f;
-  }
-}
-
-// Y = y + d of the buffer after the last fused epoch
-template <int DIM>
-__global__ void fused_final_kernel(const float* __restrict__ X, float* __restrict__ Y, int n) {
-  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  float v[DIM];
-  load_y<DIM, true>(X, (int)r, v);
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) Y[r * DIM + c] = v[c];
-}
-
 // ---- schedule ----------------------------------------------------------------
 __global__ void max_kernel(const float* __restrict__ vals, const int64_t* __restrict__ n_edges, float* __restrict__ wmax) {
   const int64_t E = *n_edges;
@@ -250,7 +151,7 @@ __global__ void eps_kernel(const float* __restrict__ vals, const int64_t* __rest
 // segment of edges, advances the schedule of the due ones and queues them in
 // shared memory; the warp works through the queue 32 edges at a time with every
 // lane busy (at most one partial batch per warp, at the end of its segment).
-template <int DIM, bool FUSED>
+template <int DIM>
 __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* __restrict__ dY, int n,
                                             const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
                                             int64_t e, int epoch, const Params& p, int neg_rate, uint32_t k0,
@@ -265,11 +166,11 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
     if (neg_rate > 4) r1 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 1u}, k0, k1);
     const uint32_t rr[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
     float yt[8][DIM];
-    load_y<DIM, FUSED>(Y, i, yi);
-    load_y<DIM, FUSED>(Y, j, yj);
+    load_row<DIM>(Y, i, yi);
+    load_row<DIM>(Y, j, yj);
 #pragma unroll
     for (int u = 0; u < 8; ++u)
-      if (u < neg_rate) load_y<DIM, FUSED>(Y, to_range(rr[u], (uint32_t)n), yt[u]);
+      if (u < neg_rate) load_row<DIM>(Y, to_range(rr[u], (uint32_t)n), yt[u]);
     attract<DIM>(yi, yj, p, pos);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
@@ -279,22 +180,22 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
 #pragma unroll
     for (int u = 0; u < 8; ++u)
       if (u < neg_rate) repel_add<DIM>(yi, yt[u], p, acc);
-    add_move<DIM, FUSED>(dY, j, neg_pos);
-    add_move<DIM, FUSED>(dY, i, acc);
+    atomic_add_row<DIM>(dY, j, neg_pos);
+    atomic_add_row<DIM>(dY, i, acc);
     return;
   }
-  load_y<DIM, FUSED>(Y, i, yi);
-  load_y<DIM, FUSED>(Y, j, yj);
+  load_row<DIM>(Y, i, yi);
+  load_row<DIM>(Y, j, yj);
   attract<DIM>(yi, yj, p, pos);
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
     acc[c] = pos[c];
     neg_pos[c] = -pos[c];
   }
-  add_move<DIM, FUSED>(dY, j, neg_pos);
+  atomic_add_row<DIM>(dY, j, neg_pos);
   auto repel = [&](uint32_t r) {
     float yt[DIM];
-    load_y<DIM, FUSED>(Y, to_range(r, (uint32_t)n), yt);
+    load_row<DIM>(Y, to_range(r, (uint32_t)n), yt);
     repel_add<DIM>(yi, yt, p, acc);
   };
 #pragma unroll 1
@@ -305,21 +206,16 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
     if (m0 + 2 < neg_rate) repel(r.z);
     if (m0 + 3 < neg_rate) repel(r.w);
   }
-  add_move<DIM, FUSED>(dY, i, acc);
+  atomic_add_row<DIM>(dY, i, acc);
 }
 
-// FUSED: Y is X_t, dY is X_{t+1} and Xz is X_{t+2} of the fused layout (the rows'
-// fold runs first); otherwise Y holds the epoch-start coordinates and dY the moves.
-template <int DIM, bool FUSED>
-__global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY,
-                                                           float* __restrict__ Xz, int n,
+template <int DIM>
+__global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY, int n,
                                                            const int32_t* __restrict__ rows,
                                                            const int32_t* __restrict__ cols,
                                                            const float* __restrict__ eps, float* __restrict__ next,
                                                            const int64_t* __restrict__ n_edges, int epoch, Params p,
                                                            int neg_rate, uint32_t k0, uint32_t k1) {
-  if constexpr (FUSED)
-    fold_rows<DIM>(Y, dY, Xz, n, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
   __shared__ int32_t queue[kBlock / 32][64];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int32_t* q = queue[warp];
@@ -349,10 +245,10 @@ __global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(co
       if (lane < cnt - 32) q[lane] = q[lane + 32];
       cnt -= 32;
       __syncwarp();
-      edge_update<DIM, FUSED>(Y, dY, n, rows, cols, my, epoch, p, neg_rate, k0, k1);
+      edge_update<DIM>(Y, dY, n, rows, cols, my, epoch, p, neg_rate, k0, k1);
     }
   }
-  if (lane < cnt) edge_update<DIM, FUSED>(Y, dY, n, rows, cols, e0 + q[lane], epoch, p, neg_rate, k0, k1);
+  if (lane < cnt) edge_update<DIM>(Y, dY, n, rows, cols, e0 + q[lane], epoch, p, neg_rate, k0, k1);
 }
 
 __global__ void apply_kernel(float* __restrict__ Y, float* __restrict__ dY, int64_t m) {
@@ -584,7 +480,6 @@ __global__ void __launch_bounds__(kBlock) sgd_injected_wide_kernel(
 struct Layout {
   int32_t* status;
   float* dY;
-  float* X[3];  // fused epochs (dim <= 4): rotating [y | d] row buffers
   float* wmax;
   int32_t* block_counts;
   int64_t* total;
@@ -597,8 +492,6 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap) {
   l.status = c.take<int32_t>(64);
   l.wmax = c.take<float>(64);
   l.dY = c.take<float>((size_t)n * dim);
-  const int fp = dim == 1 ? 2 : (dim == 2 ? 4 : 8);
-  for (int b = 0; b < 3; ++b) l.X[b] = dim <= 4 ? c.take<float>((size_t)n * fp) : nullptr;
   l.block_counts = c.take<int32_t>((size_t)ceil_div(e_cap > 0 ? e_cap : 1, kEdgesPerBlock) + 1);
   l.total = c.take<int64_t>(8);
   l.bytes = c.bytes();
@@ -633,34 +526,12 @@ template <int DIM>
 static void launch_epoch(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
                          const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
                          const Params& p, int neg_rate, uint64_t seed, cudaStream_t stream) {
-  sgd_epoch_kernel<DIM, false><<<epoch_grid(e_cap), kBlock, 0, stream>>>(
-      Y, l.dY, nullptr, (int)n, rows, cols, eps, next, n_edges, epoch, p, neg_rate, (uint32_t)seed,
-      (uint32_t)(seed >> 32));
+  sgd_epoch_kernel<DIM><<<epoch_grid(e_cap), kBlock, 0, stream>>>(Y, l.dY, (int)n, rows, cols, eps, next, n_edges,
+                                                                 epoch, p, neg_rate, (uint32_t)seed,
+                                                                 (uint32_t)(seed >> 32));
   const int64_t m = n * DIM;
   const unsigned gb = (unsigned)(ceil_div(m, kBlock) < num_sms() * 8 ? ceil_div(m, kBlock) : num_sms() * 8);
   apply_kernel<<<gb, kBlock, 0, stream>>>(Y, l.dY, m);
-}
-
-// epochs [begin, end) fused: init, one launch per epoch, final
-template <int DIM>
-static void launch_fused(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
-                         const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int begin, int end,
-                         float a, float b, float lr, int n_epochs, int neg_rate, uint64_t seed, cudaStream_t stream) {
-  const unsigned rb = (unsigned)ceil_div(n, kBlock);
-  fused_init_kernel<DIM><<<rb, kBlock, 0, stream>>>(Y, l.X[0], l.X[1], (int)n);
-  for (int ep = begin; ep < end; ++ep) {
-    const int k = ep - begin;
-    const Params p = make_params(a, b, lr, ep, n_epochs);
-    sgd_epoch_kernel<DIM, true><<<epoch_grid(e_cap), kBlock, 0, stream>>>(
-        l.X[k % 3], l.X[(k + 1) % 3], l.X[(k + 2) % 3], (int)n, rows, cols, eps, next, n_edges, ep, p, neg_rate,
-        (uint32_t)seed, (uint32_t)(seed >> 32));
-  }
-  fused_final_kernel<DIM><<<rb, kBlock, 0, stream>>>(l.X[(end - begin) % 3], Y, (int)n);
-}
-
-static bool fused_enabled() {
-  const char* e = getenv("UMAPB_LAYOUT_FUSED");
-  return !(e && e[0] == '0' && e[1] == 0);
 }
 
 static void launch_epoch_wide(const Layout& l, float* Y, int64_t n, int dim, const int32_t* rows,
@@ -734,17 +605,6 @@ static int enqueue_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows,
   if (!workspace || workspace_bytes < l.bytes)
     return set_error(UMAPB_ERR_WORKSPACE, "layout: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
   l = layout::carve(workspace, n, dim, e_cap);
-  if (dim <= 4 && layout::fused_enabled()) {
-    switch (dim) {
-      case 1: layout::launch_fused<1>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, a, b, learning_rate, n_epochs, neg_rate, seed, stream); break;
-      case 2: layout::launch_fused<2>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, a, b, learning_rate, n_epochs, neg_rate, seed, stream); break;
-      case 3: layout::launch_fused<3>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, a, b, learning_rate, n_epochs, neg_rate, seed, stream); break;
-      default: layout::launch_fused<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, epoch_begin, epoch_end, a, b, learning_rate, n_epochs, neg_rate, seed, stream); break;
-    }
-    UMAPB_LAUNCH_CHECK("layout_epochs kernels");
-    count_launches(2 + (epoch_end - epoch_begin));
-    return UMAPB_OK;
-  }
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epochs: reset");
   for (int ep = epoch_begin; ep < epoch_end; ++ep) {
     const layout::Params p = layout::make_params(a, b, learning_rate, ep, n_epochs);

@@ -96,8 +96,11 @@ __global__ void split_cols_kernel(const float* __restrict__ S, int64_t rows, int
 // ---- stable radix sort of float keys --------------------------------------------
 constexpr int kSortTile = 1024;
 
+// order-preserving unsigned image of a float; -0.0 maps with +0.0 (they compare
+// equal, so the stable sort keeps them in index order)
 __device__ __forceinline__ uint32_t f2ord(float f) {
-  const uint32_t u = __float_as_uint(f);
+  uint32_t u = __float_as_uint(f);
+  if (u == 0x80000000u) u = 0u;
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
 
@@ -275,9 +278,9 @@ __global__ void sum_slices_kernel(const float* __restrict__ C, int slices, int64
                                   float* __restrict__ out) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
-  float s = C[t];
-  for (int z = 1; z < slices; ++z) s = __fadd_rn(s, C[(int64_t)z * count + t]);
-  out[t] = __fmul_rn(s, scale);
+  double s = 0.0;  // FP64: the slices' FP32 partial sums add without further rounding drift
+  for (int z = 0; z < slices; ++z) s += (double)C[(int64_t)z * count + t];
+  out[t] = (float)(s * (double)scale);
 }
 }  // namespace linalg
 }  // namespace umapb
