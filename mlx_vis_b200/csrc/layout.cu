@@ -42,6 +42,7 @@ constexpr int kEdgesPerBlock = 1024;
 #endif
 // resident blocks per SM the epoch kernel is compiled for (register cap) and launched with
 constexpr int kEpochBlocksPerSM = UMAPB_LAYOUT_BLOCKS_PER_SM;
+constexpr int kPre = 8;  // epoch kernel: chunks of 32 edges whose schedule words load together
 
 // ---- reference pair math (float32, evaluation order of umap.py:361-383) ----
 struct Params {
@@ -216,39 +217,50 @@ __global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(co
                                                            const float* __restrict__ eps, float* __restrict__ next,
                                                            const int64_t* __restrict__ n_edges, int epoch, Params p,
                                                            int neg_rate, uint32_t k0, uint32_t k1) {
-  __shared__ int32_t queue[kBlock / 32][64];
+  // A pass: every warp loads the schedule words of kPre chunks of 32 edges of its
+  // segment at once (one round trip instead of kPre), advances the due edges and
+  // appends them to the block's queue; then the block's 8 warps take the queue 32
+  // edges at a time, so only the block's last batch of the pass runs partly empty.
+  __shared__ int32_t bq[(kBlock / 32) * kPre * 32];
+  __shared__ int s_cnt;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int32_t* q = queue[warp];
   const int64_t E = *n_edges;
   const float ep = (float)epoch;
   const int64_t n_warps = (int64_t)gridDim.x * (kBlock / 32);
   const int64_t seg = (((E + 31) / 32 + n_warps - 1) / n_warps) * 32;
-  const int64_t e0 = ((int64_t)blockIdx.x * (kBlock / 32) + warp) * seg;
+  const int64_t b0 = (int64_t)blockIdx.x * (kBlock / 32) * seg;
+  const int64_t e0 = b0 + (int64_t)warp * seg;
   const int64_t e1 = e0 + seg < E ? e0 + seg : E;
   const unsigned below = (1u << lane) - 1u;
-  int cnt = 0;  // queued edges (offsets from e0), < 32 between batches
-  for (int64_t base = e0; base < e1; base += 32) {
-    const int64_t e = base + lane;
-    bool due = false;
-    if (e < e1) {
-      const float nx = next[e];
-      due = nx <= ep;
-      if (due) next[e] = __fadd_rn(nx, eps[e]);
+  const int passes = (int)((seg + 32 * kPre - 1) / (32 * kPre));  // the same for every warp of the grid
+  for (int ps = 0; ps < passes; ++ps) {
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const int64_t sb = e0 + (int64_t)ps * 32 * kPre;
+    float nx[kPre], ex[kPre];
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int64_t e = sb + 32 * u + lane;
+      nx[u] = e < e1 ? next[e] : INFINITY;
+      ex[u] = e < e1 ? eps[e] : 0.f;
     }
-    const unsigned b = __ballot_sync(0xffffffffu, due);
-    if (due) q[cnt + __popc(b & below)] = (int32_t)(e - e0);
-    cnt += __popc(b);
-    __syncwarp();
-    if (cnt >= 32) {
-      const int64_t my = e0 + q[lane];
-      __syncwarp();
-      if (lane < cnt - 32) q[lane] = q[lane + 32];
-      cnt -= 32;
-      __syncwarp();
-      edge_update<DIM>(Y, dY, n, rows, cols, my, epoch, p, neg_rate, k0, k1);
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int64_t e = sb + 32 * u + lane;
+      const bool due = nx[u] <= ep;
+      if (due) next[e] = __fadd_rn(nx[u], ex[u]);
+      const unsigned b = __ballot_sync(0xffffffffu, due);
+      int slot = 0;
+      if (lane == 0 && b) slot = atomicAdd(&s_cnt, __popc(b));
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if (due) bq[slot + __popc(b & below)] = (int32_t)(e - b0);
     }
+    __syncthreads();
+    const int total = s_cnt;
+    for (int base = warp * 32; base < total; base += kBlock)
+      if (base + lane < total) edge_update<DIM>(Y, dY, n, rows, cols, b0 + bq[base + lane], epoch, p, neg_rate, k0, k1);
+    __syncthreads();
   }
-  if (lane < cnt) edge_update<DIM>(Y, dY, n, rows, cols, e0 + q[lane], epoch, p, neg_rate, k0, k1);
 }
 
 __global__ void apply_kernel(float* __restrict__ Y, float* __restrict__ dY, int64_t m) {
