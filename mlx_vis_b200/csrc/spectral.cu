@@ -375,20 +375,44 @@ __global__ void __launch_bounds__(kBlock) power_kernel(float* __restrict__ V0, f
 #pragma unroll
       for (int j = 0; j < kk; ++j) acc[j] = 0.0;
       const int64_t e1 = valid ? row_ptr[r + 1] : 0;
-      for (int64_t e = valid ? row_ptr[r] + sub : 0; e < e1; e += kLanes) {
-        const int64_t c = cols[e];
-        const double w = (double)wn[e];
+      // one edge's contribution: acc_j += w q_j with q_j = sum_i v_i Rinv[i][j]
+      auto add_edge = [&](double w, const float4& a, float a4) {
         double v[kMaxCols];
-        const float4 a = __ldcg(reinterpret_cast<const float4*>(Vin + c * vp));  // rows padded to 4 or 8
         v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
-        if (kk > 4) v[4] = __ldcg(Vin + c * vp + 4);
+        if (kk > 4) v[4] = a4;
 #pragma unroll
-        for (int j = 0; j < kk; ++j) {  // q_j = sum_i v_i Rinv[i][j]
+        for (int j = 0; j < kk; ++j) {
           double q = 0.0;
 #pragma unroll
           for (int i = 0; i <= j; ++i) q += v[i] * ri[i * kk + j];
           acc[j] += w * q;
         }
+      };
+      int64_t e = valid ? row_ptr[r] + sub : 0;
+      // four edges per step: their column ids, weights and V rows are loaded
+      // together (two round trips per four edges); the sums keep edge order
+      for (; e + 3 * kLanes < e1; e += 4 * kLanes) {
+        int64_t c[4];
+        double w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          c[u] = cols[e + u * kLanes];
+          w[u] = (double)wn[e + u * kLanes];
+        }
+        float4 a[4];
+        float a4[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          a[u] = __ldcg(reinterpret_cast<const float4*>(Vin + c[u] * vp));  // rows padded to 4 or 8
+          a4[u] = kk > 4 ? __ldcg(Vin + c[u] * vp + 4) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) add_edge(w[u], a[u], a4[u]);
+      }
+      for (; e < e1; e += kLanes) {
+        const int64_t c = cols[e];
+        add_edge((double)wn[e], __ldcg(reinterpret_cast<const float4*>(Vin + c * vp)),
+                 kk > 4 ? __ldcg(Vin + c * vp + 4) : 0.f);
       }
 #pragma unroll
       for (int j = 0; j < kk; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 1);  // kLanes == 2
