@@ -657,9 +657,6 @@ __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
   }
 }
 
-// row kernel: candidate chunks of 32 whose loads are issued together (T <= 256)
-constexpr int kPreChunks = 8;
-
 // dedup hash (4 hcap bytes), later candidate distances (4 tcap) + to-do list (2 tcap)
 __host__ __device__ inline size_t iter_scratch_bytes(int tcap, int hcap) {
   const size_t a = (size_t)hcap * 4, b = (size_t)tcap * 6;
@@ -742,7 +739,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   // 1. candidate ids in the reference's column order
   const int nn_cols = a.mc_new * a.j_nn;
   const int T_total = k + nn_cols + (a.rev ? k : 0);
-  auto cand_id = [&](int t) {
+  for (int t = lane; t < a.tcap; t += 32) {
     int id = 0x7fffffff;
     if (t < k) {
       id = orow[t];
@@ -753,19 +750,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
     } else if (t < T_total) {
       id = a.rev[row * k + (t - k - nn_cols)];
     }
-    return id;
-  };
-  if (a.tcap <= 32 * kPreChunks) {
-    // up to kPreChunks chunks: every chunk's loads issued before any store, one
-    // round trip instead of one per chunk
-    int ids[kPreChunks];
-#pragma unroll
-    for (int c = 0; c < kPreChunks; ++c) ids[c] = c * 32 < a.tcap ? cand_id(c * 32 + lane) : 0x7fffffff;
-#pragma unroll
-    for (int c = 0; c < kPreChunks; ++c)
-      if (c * 32 < a.tcap) cid[c * 32 + lane] = ids[c];
-  } else {
-    for (int t = lane; t < a.tcap; t += 32) cid[t] = cand_id(t);
+    cid[t] = id;
   }
   __syncwarp();
 
@@ -796,10 +781,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
 
   // 3. stored distances and the list of distances to compute
   int n_todo = 0;
-  // the stored distance of column t, or need = true when it must be computed
-  auto stored = [&](int t, int ch, bool& need) {
+  for (int t0 = 0, ch = 0; t0 < a.tcap; t0 += 32, ++ch) {
+    const int t = t0 + lane;
     float d = kBig;
-    need = false;
+    bool need = false;
     if ((keep >> ch) & 1ull) {
       if (t < k) {
         if (!a.recompute_cur) d = a.dist_old[row * k + t];
@@ -826,28 +811,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
         need = true;
       }
     }
-    return d;
-  };
-  auto append = [&](int t, float d, bool need) {
     cd[t] = d;
     const unsigned nb = __ballot_sync(0xffffffffu, need);
     if (need) todo[n_todo + __popc(nb & ((1u << lane) - 1u))] = (uint16_t)t;
     n_todo += __popc(nb);
-  };
-  if (a.tcap <= 32 * kPreChunks) {  // loads of every chunk first, then the appends
-    float dv[kPreChunks];
-    bool nd[kPreChunks];
-#pragma unroll
-    for (int c = 0; c < kPreChunks; ++c) dv[c] = c * 32 < a.tcap ? stored(c * 32 + lane, c, nd[c]) : (nd[c] = false, kBig);
-#pragma unroll
-    for (int c = 0; c < kPreChunks; ++c)
-      if (c * 32 < a.tcap) append(c * 32 + lane, dv[c], nd[c]);
-  } else {
-    for (int t0 = 0, ch = 0; t0 < a.tcap; t0 += 32, ++ch) {
-      bool need;
-      const float d = stored(t0 + lane, ch, need);
-      append(t0 + lane, d, need);
-    }
   }
   __syncwarp();
   const float sqi = a.sqd[row];
