@@ -162,7 +162,18 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     With a workspace (size from the _workspace query) the draws
  *                     run grid-wide on words generated ahead with a 10-sigma
  *                     margin (a shortfall is redone on the device by one CTA);
- *                     without one, one CTA walks the stream.
+ *                     without one, one CTA walks the stream.  Streams longer than
+ *                     86,720 words are generated in segments of 65,536 words on
+ *                     separate CTAs, each started by jumping ahead; the first such
+ *                     call per device copies the jump polynomials to the device
+ *                     and synchronises the stream once (under stream capture the
+ *                     call generates on one CTA instead).
+ * umapb_mt_jump_poly: host only (no GPU needed), for tests and other hosts: the
+ *                     jump polynomial x^D mod phi for D = b * 65536 words (*words_ahead
+ *                     receives D), 1 <= b <= 1024, as 312 words (bit i of word i/64
+ *                     = coefficient of x^i); phi is MT19937's characteristic
+ *                     polynomial (degree 19937).  Raw words then satisfy
+ *                     x[n + D] = XOR over set bits i of x[n + i] for n >= 1.
  * ------------------------------------------------------------------------- */
 int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float* sq, umapb_stream_t stream);
 int umapb_nnd_to_half(const float* X, int64_t n, int32_t dd, int32_t ldh, void* H, umapb_stream_t stream);
@@ -187,6 +198,7 @@ int umapb_nnd_random_start_workspace(int64_t n, int32_t k, int32_t d, int32_t pd
 int umapb_nnd_random_start(uint32_t* state, int64_t n, int32_t k, int32_t d, int32_t* idx, float* P, int32_t pd1,
                            float* P2, int32_t pd2, void* workspace, size_t workspace_bytes,
                            umapb_stream_t stream);
+int umapb_mt_jump_poly(int32_t b, uint64_t* out, int64_t* words_ahead);
 /* umapb_legacy_normal: count values float32(loc + scale * g) with g NumPy's legacy
  * standard normals drawn from `state` (same buffer layout as above; overwritten
  * with the state after the draws) — RandomState(seed).normal(loc, scale, count)

@@ -67,6 +67,7 @@ SIGNATURES = {
     "umapb_nnd_sqrt": [_p, _i64, _p, _p],
     "umapb_nnd_random_start_workspace": [_i64, _i32, _i32, _i32, _i32, _psz],
     "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p, _sz, _p],
+    "umapb_mt_jump_poly": [_i32, _p, _c.POINTER(_i64)],
     "umapb_legacy_normal_workspace": [_i64, _psz],
     "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p, _sz, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],
@@ -258,6 +259,17 @@ def legacy_normal(rs, shape, loc: float, scale: float, device, parallel: bool = 
     call("umapb_legacy_normal", ptr(state), out.numel(), float(loc), float(scale), ptr(out), ptr(ws),
          ws.numel() if ws is not None else 0, stream_handle())
     return out
+
+
+def mt_jump_poly(b: int):
+    """(coefficients, D): x^D mod phi for D = b * 65536 as a bool array of length
+    19937 (coefficient of x^i at i), phi MT19937's characteristic polynomial; host
+    code of the library, no GPU needed (umapb_mt_jump_poly)."""
+    out = np.zeros(312, dtype=np.uint64)
+    D = _i64(0)
+    call("umapb_mt_jump_poly", int(b), out.ctypes.data, _c.byref(D))
+    bits = np.unpackbits(out.view(np.uint8), bitorder="little")[:19937].astype(bool)
+    return bits, int(D.value)
 
 
 def set_wait_limit_ns(ns: int) -> None:

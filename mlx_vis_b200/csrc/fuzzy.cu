@@ -13,7 +13,7 @@
 //               searchsorted finds, umap.py:241-260), w_sym = (w + w') - w w'
 //               in float32 without contraction; grid max of w_sym.
 // K3-K5 prune:  keep w_sym >= max / n_epochs (float32, umap.py:265-270) with an
-//               order-preserving compaction (block counts, one-block scan, write).
+//               order-preserving compaction (block counts, exclusive scan, write).
 #include <math.h>
 
 #include "common.cuh"
@@ -232,7 +232,7 @@ extern "C" int umapb_fuzzy(const int32_t* knn_idx, const float* knn_dist, int64_
   const int64_t nb = ceil_div(m, fuzzy::kEdgesPerBlock);
   fuzzy::prune_count_kernel<<<(unsigned)nb, fuzzy::kBlock, 0, stream>>>(l.w_sym, m, l.wmax, n_epochs, l.block_counts);
   UMAPB_LAUNCH_CHECK("fuzzy: prune count kernel");
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, nb, n_edges);
+  scan_exclusive(l.block_counts, nb, n_edges, stream);
   UMAPB_LAUNCH_CHECK("fuzzy: scan kernel");
   fuzzy::prune_write_kernel<<<(unsigned)nb, fuzzy::kBlock, 0, stream>>>(l.w_sym, knn_idx, m, k, l.wmax, n_epochs,
                                                                        l.block_counts, rows, cols, vals);

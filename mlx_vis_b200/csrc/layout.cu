@@ -718,7 +718,7 @@ extern "C" int umapb_layout_count_active(const float* next, const int64_t* n_edg
   l = layout::carve(workspace, n, dim, e_cap);
   const int64_t nb = ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
   layout::count_active_kernel<<<(unsigned)nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, nb, count);
+  scan_exclusive(l.block_counts, nb, count, stream);
   UMAPB_LAUNCH_CHECK("layout_count_active kernels");
   count_launches(2);
   return UMAPB_OK;
@@ -744,7 +744,7 @@ extern "C" int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, con
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epoch_injected: reset");
   const unsigned nb = (unsigned)ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
   layout::count_active_kernel<<<nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.block_counts, (int64_t)nb, l.total);
+  scan_exclusive(l.block_counts, (int64_t)nb, l.total, stream);
   UMAPB_LAUNCH_CHECK("layout_epoch_injected: active count");
   int64_t active = 0;
   UMAPB_CUDA_TRY(cudaMemcpyAsync(&active, l.total, sizeof(active), cudaMemcpyDeviceToHost, stream),

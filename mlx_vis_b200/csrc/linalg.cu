@@ -262,7 +262,7 @@ extern "C" int umapb_sort_keys(const float* keys, int64_t n, int64_t stride, int
   for (int pass = 0; pass < 4; ++pass) {
     const int src = pass & 1, dst = src ^ 1;
     linalg::sort_hist_kernel<<<(unsigned)tiles, linalg::kSortTile, 0, stream>>>(l.k[src], n, 8 * pass, l.counts);
-    scan_exclusive_kernel<<<1, 1024, 0, stream>>>(l.counts, 256 * tiles, l.total);
+    scan_exclusive(l.counts, 256 * tiles, l.total, stream);
     int32_t* iout = pass == 3 ? order : l.i[dst];
     linalg::sort_scatter_kernel<<<(unsigned)tiles, linalg::kSortTile, 0, stream>>>(
         l.k[src], l.i[src], n, 8 * pass, l.counts, l.k[dst], iout);

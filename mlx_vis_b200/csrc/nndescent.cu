@@ -993,7 +993,7 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   nnd::indegree_kernel<<<blocks, 256, 0, stream>>>(idx, m, off);
   UMAPB_CUDA_TRY(cudaMemcpyAsync(deg, off, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, stream),
                  "nnd_reverse: degree copy");
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n, total);
+  scan_exclusive(off, n, total, stream);
   nnd::bucket_fill_kernel<<<blocks, 256, 0, stream>>>(idx, m, k, off, fill, bucket);
   nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
                                                                                                   n, k, 0, rev);
@@ -1055,7 +1055,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   const int64_t want = ceil_div(m, 256);
   const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
   nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off);
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(off, n + 1, total);
+  scan_exclusive(off, n + 1, total, stream);
   nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off, fill, entries);
   if (rev_out) {  // with mc == k the buckets are the reverse-candidate buckets
     nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(
@@ -1064,7 +1064,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   const unsigned sblocks = (unsigned)ceil_div(n, 256);
   UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
   nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, order, n, choff);
-  scan_exclusive_kernel<<<1, 1024, 0, stream>>>(choff, n + 1, total);
+  scan_exclusive(choff, n + 1, total, stream);
   nnd::chunk_fill_kernel<<<sblocks, 256, 0, stream>>>(choff, n, chunk_pos);
   nnd::JoinArgs a;
   a.Xd = Xd;

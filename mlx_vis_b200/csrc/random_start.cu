@@ -10,9 +10,10 @@
 // 53-bit doubles.  Every output depends on how many words the rejections before
 // it consumed.
 //
-// Parallel path (with a workspace): one CTA only runs the MT recurrence and
-// stores the raw state of every generation, enough words for the requested
-// counts with a 10-sigma margin on the rejections; the acceptance tests, ranks
+// Parallel path (with a workspace): the MT recurrence runs first and stores the
+// raw state of every generation, enough words for the requested counts with a
+// 10-sigma margin on the rejections (one CTA for short streams; segments of 65,536
+// words on separate CTAs, started by jump-ahead, for long ones); the acceptance tests, ranks
 // (block counts + scan) and output scatter then run over the whole grid, first
 // for the integers, then for the normal pairs starting at the word where the
 // integers stopped.  A final kernel rebuilds NumPy's state at the word where the
@@ -26,6 +27,9 @@
 // first), NumPy's get_state() layout.  No waits: every loop ends when the
 // requested counts are produced or the generated words run out.
 #include <math.h>
+
+#include <mutex>
+#include <vector>
 
 #include "common.cuh"
 #include "scan.cuh"
@@ -267,43 +271,151 @@ struct Scalars {
 //                   ^ mix(x_{n-624}, x_{n-623}),
 // whose nearest operand is 623 words back: a block of 623 words depends only on
 // earlier blocks, so one barrier covers 623 words (the plain recurrence allows 227).
-// Words 624..1077 use the plain recurrence in two blocks of 227.  A block writes
-// ring slots n mod 2048 that none of its reads touch (those lie 456..1700 slots
-// away), so every block costs one barrier.
+// A run that starts at word n0 from the 624 words before it uses the plain
+// recurrence for its first 454 words (two blocks of 227), then blocks of 623.  A
+// block writes ring slots n mod 2048 that none of its reads touch (those lie
+// 456..1700 slots away), so every block costs one barrier.
+//
+// One CTA generates about 3 words per ns, bound by its own instructions; longer
+// streams are cut into segments of kSeg words that run on separate CTAs, each
+// started from the 624 words before it, computed by jumping ahead:
+//
+// Jump-ahead.  Every bit position of x_n follows a linear recurrence over GF(2)
+// whose characteristic polynomial is the generator's, phi, of degree 19937
+// (Matsumoto & Nishimura 1998).  With r(x) = x^D mod phi(x) = sum_i r_i x^i,
+//   x_{n+D} = XOR over {i : r_i = 1} of x_{n+i}     for every n >= 1
+// (the low 31 bits of x_0 never enter the recurrence, hence n >= 1).  r depends on
+// D only, not on the seed, so the host computes phi once (Berlekamp-Massey on one
+// output bit of the generator) and the polynomials r for D = b kSeg (repeated
+// multiplication by x^16384 reduced mod phi, whose terms below the leading one
+// lie at least 623 exponents lower, so the reduction proceeds 64 bits at a time).
+// On the device the 624 words that start segment b are XORs over a window of
+// 19937 + 623 words that one CTA generated first.
 constexpr int kStreamThreads = 640;
 constexpr int kWide = 623;
 constexpr int kRing = 2048;
+constexpr int kDeg = 19937;                        // degree of phi
+constexpr int kPolyWords = (kDeg + 63) / 64;       // 312 64-bit words per jump polynomial
+constexpr int64_t kSeg = 65536;                    // words per segment
+constexpr int kMaxJumps = 1024;                    // jump polynomials kept: segments 1..1024
+constexpr int64_t kWinEnd = kN + (kDeg - 1) + kN;  // the window is x_624 .. x_21183
+constexpr int kJumpParts = 32;                     // CTAs per segment start, one exponent range each
+constexpr int kPartBits = 640;                     // exponents per CTA (10 polynomial words)
+constexpr int kJumpThreads = 160;                  // a thread XORs words w, w + 160, w + 320, w + 480
+static_assert(kJumpParts * kPartBits >= kDeg && kPartBits % 64 == 0, "jump ranges cover phi");
 
-__global__ void __launch_bounds__(kStreamThreads) stream_kernel(const uint32_t* __restrict__ state, int64_t total,
+// row b - 1: x^(b kSeg) mod phi, bit i of word i / 64 = coefficient of x^i
+__device__ uint64_t g_jump_poly[(size_t)kMaxJumps * kPolyWords];
+
+// Words n0 .. end - 1; the ring holds x_{n0-624} .. x_{n0-1} at slots n mod 2048 and
+// the caller has synchronised after filling it.
+__device__ __forceinline__ void gen_words(uint32_t* ring, int64_t n0, int64_t end, uint32_t* __restrict__ raw) {
+  constexpr uint32_t R = kRing - 1;
+  const int t = threadIdx.x;
+  const int64_t wide0 = n0 + 2 * kHalf;
+  for (int64_t base = n0; base < wide0 && base < end; base += kHalf) {
+    const int64_t n = base + t;
+    if (t < kHalf && n < end) {
+      const uint32_t m = (uint32_t)n;
+      const uint32_t x = ring[(m - kHalf) & R] ^ mix(ring[(m - kN) & R], ring[(m - kN + 1) & R]);
+      ring[m & R] = x;
+      raw[n] = x;
+    }
+    __syncthreads();
+  }
+  for (int64_t base = wide0; base < end; base += kWide) {
+    const int64_t n = base + t;
+    if (t < kWide && n < end) {
+      const uint32_t m = (uint32_t)n;
+      const uint32_t x = ring[(m - 681) & R] ^ mix(ring[(m - 1078) & R], ring[(m - 1077) & R]) ^
+                         mix(ring[(m - 851) & R], ring[(m - 850) & R]) ^ mix(ring[(m - 624) & R], ring[(m - 623) & R]);
+      ring[m & R] = x;
+      raw[n] = x;
+    }
+    __syncthreads();
+  }
+}
+
+// raw[0 .. end): the incoming key, then x_624 .. x_{end-1}
+__global__ void __launch_bounds__(kStreamThreads) stream_kernel(const uint32_t* __restrict__ state, int64_t end,
                                                                 uint32_t* __restrict__ raw) {
   __shared__ uint32_t ring[kRing];
-  constexpr int R = kRing - 1;
-  const int t = threadIdx.x;
-  for (int i = t; i < kN; i += kStreamThreads) {
+  for (int i = threadIdx.x; i < kN; i += kStreamThreads) {
     const uint32_t v = state[i];
     ring[i] = v;
     raw[i] = v;
   }
   __syncthreads();
-  for (int64_t base = kN; base < 1078 && base < total; base += kHalf) {
-    const int64_t n = base + t;
-    if (t < kHalf && n < total) {
-      const uint32_t x = ring[(n - kHalf) & R] ^ mix(ring[(n - kN) & R], ring[(n - kN + 1) & R]);
-      ring[n & R] = x;
-      raw[n] = x;
+  gen_words(ring, kN, end, raw);
+}
+
+// Partial start words of segment b = 1 + blockIdx.x / kJumpParts over the exponents
+// [g kPartBits, (g + 1) kPartBits) of its polynomial, g = blockIdx.x % kJumpParts:
+// part[(b - 1, g, w)] = XOR over those set exponents i of x_{624 + i + w}, w < 624.
+__global__ void __launch_bounds__(kJumpThreads) jump_kernel(const uint32_t* __restrict__ raw,
+                                                            uint32_t* __restrict__ part) {
+  constexpr int kWinWords = kPartBits + 4 * kJumpThreads - 1;  // w up to 639 (words past 623 are unused)
+  __shared__ uint32_t win[kWinWords];
+  __shared__ uint16_t list[kPartBits];  // the set exponents, minus i0
+  __shared__ int s_cnt;
+  const int b1 = blockIdx.x / kJumpParts, g = blockIdx.x % kJumpParts;
+  const int i0 = g * kPartBits;
+  const int i1 = min(kDeg, i0 + kPartBits);
+  const int t = threadIdx.x;
+  const int have = i1 - i0 + kN - 1;  // x_{624 + i0} .. x_{624 + i1 + 622}, inside the window
+  for (int u = t; u < kWinWords; u += kJumpThreads) win[u] = u < have ? raw[kN + i0 + u] : 0u;
+  if (t < 32) {  // warp 0 lists the set exponents in increasing order (none at or past kDeg)
+    const uint32_t* poly32 = reinterpret_cast<const uint32_t*>(g_jump_poly + (size_t)b1 * kPolyWords);
+    int cnt = 0;
+    for (int c = 0; c < kPartBits / 32; ++c) {
+      const int q = i0 / 32 + c;
+      const uint32_t word = q < 2 * kPolyWords ? poly32[q] : 0u;  // little-endian halves of the 64-bit words
+      const bool set = (word >> t) & 1u;
+      const unsigned bal = __ballot_sync(0xffffffffu, set);
+      if (set) list[cnt + __popc(bal & ((1u << t) - 1u))] = (uint16_t)(c * 32 + t);
+      cnt += __popc(bal);
     }
-    __syncthreads();
+    if (t == 0) s_cnt = cnt;
   }
-  for (int64_t base = 1078; base < total; base += kWide) {
-    const int64_t n = base + t;
-    if (t < kWide && n < total) {
-      const uint32_t x = ring[(n - 681) & R] ^ mix(ring[(n - 1078) & R], ring[(n - 1077) & R]) ^
-                         mix(ring[(n - 851) & R], ring[(n - 850) & R]) ^ mix(ring[(n - 624) & R], ring[(n - 623) & R]);
-      ring[n & R] = x;
-      raw[n] = x;
+  __syncthreads();
+  const int cnt = s_cnt;
+  uint32_t acc[4] = {0u, 0u, 0u, 0u};
+#pragma unroll 4
+  for (int s = 0; s < cnt; ++s) {
+    const int i = list[s];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc[u] ^= win[i + t + u * kJumpThreads];  // i + w < kWinWords
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int w = t + u * kJumpThreads;
+    if (w < kN) part[((size_t)b1 * kJumpParts + g) * kN + w] = acc[u];
+  }
+}
+
+// Segment b = blockIdx.x generates x_n for n in [1248 + b kSeg, 1248 + (b + 1) kSeg)
+// (the last one up to `total`) from x_{624 + b kSeg} .. x_{1247 + b kSeg}: for b = 0
+// the window's words, else the XOR of the segment's kJumpParts partial words.
+__global__ void __launch_bounds__(kStreamThreads) segment_kernel(const uint32_t* __restrict__ part, int64_t total,
+                                                                 int nseg, uint32_t* __restrict__ raw) {
+  __shared__ uint32_t ring[kRing];
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int64_t s0 = kN + (int64_t)b * kSeg;
+  const int64_t n0 = s0 + kN;
+  const int64_t end = b == nseg - 1 ? total : min(total, n0 + kSeg);
+  if (t < kN) {
+    uint32_t v = 0u;
+    if (b == 0) {
+      v = raw[s0 + t];
+    } else {
+      const uint32_t* p = part + (size_t)(b - 1) * kJumpParts * kN + t;
+#pragma unroll 8
+      for (int g = 0; g < kJumpParts; ++g) v ^= p[(size_t)g * kN];
     }
-    __syncthreads();
+    ring[(uint32_t)(s0 + t) & (kRing - 1)] = v;
   }
+  __syncthreads();
+  gen_words(ring, n0, end, raw);
 }
 
 // exclusive prefix of v over the block (kPar threads) and the block total
@@ -471,12 +583,193 @@ __global__ void const_ints_kernel(int64_t count, int k, int32_t* __restrict__ id
     idx[q] = (q / k) == 0 ? 1 : 0;
 }
 
+// ---- jump polynomials (host) ---------------------------------------------------
+namespace jumps {
+constexpr int kShift = 16384;                   // x^kSeg = (x^kShift)^4
+constexpr int kBuf = (kDeg + kShift) / 64 + 2;  // words of a product before its reduction
+constexpr int kMaxDev = 64;
+
+inline uint32_t mix_h(uint32_t a, uint32_t b) {
+  const uint32_t y = (a & kUpper) | (b & kLower);
+  return (y >> 1) ^ ((y & 1u) ? kMatrixA : 0u);
+}
+
+// bits [pos, pos + 64) of a bit array, zero past its end
+inline uint64_t get64(const std::vector<uint64_t>& a, int64_t pos) {
+  const size_t q = (size_t)(pos >> 6);
+  const int s = (int)(pos & 63);
+  const uint64_t lo = q < a.size() ? a[q] : 0ull;
+  const uint64_t hi = q + 1 < a.size() ? a[q + 1] : 0ull;
+  return s ? (lo >> s) | (hi << (64 - s)) : lo;
+}
+
+// C ^= B x^m (terms past C's end are zero by the callers' degree bounds)
+inline void xor_shift(std::vector<uint64_t>& C, const std::vector<uint64_t>& B, int m) {
+  const int a = m >> 6, s = m & 63;
+  for (int q = (int)C.size() - 1; q >= a; --q) {
+    uint64_t v = B[q - a] << s;
+    if (s && q - a - 1 >= 0) v |= B[q - a - 1] >> (64 - s);
+    C[q] ^= v;
+  }
+}
+
+// phi by Berlekamp-Massey (Massey 1969) on the top bit of 2 kDeg + 64 raw words of
+// the recurrence from an arbitrary state.  exps: phi's exponents below kDeg, in
+// decreasing order.  Fails unless the linear complexity is kDeg, phi(0) = 1 and the
+// highest exponent below kDeg is at least 64 lower (the reduction's step).
+bool char_poly(std::vector<int>& exps) {
+  constexpr int N = 2 * kDeg + 64;
+  constexpr int skip = 4 * kN;
+  std::vector<uint32_t> x((size_t)kN + skip + N);
+  uint32_t v = 2463534242u;  // xorshift32 (Marsaglia 2003) fills the first generation
+  for (int i = 0; i < kN; ++i) {
+    v ^= v << 13;
+    v ^= v >> 17;
+    v ^= v << 5;
+    x[i] = v;
+  }
+  for (size_t n = kN; n < x.size(); ++n) x[n] = x[n - kHalf] ^ mix_h(x[n - kN], x[n - kN + 1]);
+  const int words = N / 64 + 4;
+  std::vector<uint64_t> rv(words, 0ull);  // bit j = s_{N-1-j}, s_j = top bit of x_{624 + skip + j}
+  for (int j = 0; j < N; ++j)
+    if (x[(size_t)kN + skip + j] >> 31) {
+      const int p = N - 1 - j;
+      rv[p >> 6] |= 1ull << (p & 63);
+    }
+  std::vector<uint64_t> C(words, 0ull), B(words, 0ull), T;
+  C[0] = B[0] = 1ull;
+  int L = 0, m = 1;
+  for (int n = 0; n < N; ++n) {
+    const int64_t base = (int64_t)N - 1 - n;  // rv bit of s_n; s_{n-i} is bit base + i
+    uint64_t d = 0ull;
+    for (int q = 0; q <= L / 64; ++q) d ^= C[q] & get64(rv, base + 64 * q);
+    if ((__builtin_popcountll(d) & 1) == 0) {
+      ++m;
+    } else if (2 * L <= n) {
+      T = C;
+      xor_shift(C, B, m);
+      L = n + 1 - L;
+      B.swap(T);
+      m = 1;
+    } else {
+      xor_shift(C, B, m);
+      ++m;
+    }
+  }
+  if (L != kDeg || !((C[L >> 6] >> (L & 63)) & 1ull)) return false;
+  exps.clear();
+  for (int i = 1; i <= L; ++i)  // phi(x) = x^L C(1/x): coefficient of x^(L - i) is c_i
+    if ((C[i >> 6] >> (i & 63)) & 1ull) exps.push_back(L - i);
+  return !exps.empty() && exps.back() == 0 && exps.front() <= kDeg - 64;
+}
+
+inline void xor_at(uint64_t* w, int pos, uint64_t v) {
+  if (pos < 0) {  // only the partial top word: its bits below -pos are zero
+    v >>= -pos;
+    pos = 0;
+  }
+  const int q = pos >> 6, s = pos & 63;
+  w[q] ^= v << s;
+  if (s) w[q + 1] ^= v >> (64 - s);
+}
+
+// w <- w x^s mod phi for w of degree < kDeg (kBuf words), s <= kShift.  The top
+// 64-bit word above x^kDeg folds down through x^kDeg = sum of x^e over exps: every
+// image lies at least 623 - 63 bits below the word, so one pass from the top works.
+void mulx_mod(uint64_t* w, int s, const std::vector<int>& exps) {
+  const int a = s >> 6, b = s & 63;
+  for (int q = kBuf - 1; q >= 0; --q) {
+    uint64_t v = q - a >= 0 ? w[q - a] << b : 0ull;
+    if (b && q - a - 1 >= 0) v |= w[q - a - 1] >> (64 - b);
+    w[q] = v;
+  }
+  for (int q = kBuf - 1; q >= kDeg / 64; --q) {
+    uint64_t v = w[q];
+    if (q == kDeg / 64) v &= ~0ull << (kDeg & 63);
+    if (!v) continue;
+    w[q] ^= v;
+    for (int e : exps) xor_at(w, 64 * q - kDeg + e, v);
+  }
+}
+
+struct Table {
+  std::mutex mu;
+  bool tried = false, ok = false;
+  std::vector<int> exps;
+  std::vector<uint64_t> cur;    // x^(count kSeg) mod phi, kBuf words
+  std::vector<uint64_t> polys;  // count rows of kPolyWords: x^(b kSeg) mod phi, b = 1..count
+  int count = 0;
+  int uploaded[kMaxDev] = {};   // rows in each device's g_jump_poly
+};
+
+Table& table() {
+  static Table t;
+  return t;
+}
+
+// the first `need` rows on the host; the caller holds the lock
+bool extend(Table& T, int need) {
+  if (!T.tried) {
+    T.tried = true;
+    T.ok = char_poly(T.exps);
+    if (T.ok) {
+      T.cur.assign(kBuf, 0ull);
+      T.cur[0] = 1ull;
+    }
+  }
+  if (!T.ok) return false;
+  while (T.count < need) {
+    for (int s = 0; s < kSeg / kShift; ++s) mulx_mod(T.cur.data(), kShift, T.exps);
+    T.polys.insert(T.polys.end(), T.cur.begin(), T.cur.begin() + kPolyWords);
+    ++T.count;
+  }
+  return true;
+}
+}  // namespace jumps
+
+// Rows 1..need of g_jump_poly on the current device.  A first upload (one per device
+// and table size) is synchronised on `stream`, so it is skipped, and the one-CTA
+// stream used instead, while the stream is being captured.
+static bool jump_table_ready(int need, cudaStream_t stream) {
+  int dev = 0;
+  if (need < 1 || need > kMaxJumps || cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= jumps::kMaxDev)
+    return false;
+  jumps::Table& T = jumps::table();
+  std::lock_guard<std::mutex> lock(T.mu);
+  if (!jumps::extend(T, need)) return false;
+  if (T.uploaded[dev] >= need) return true;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    return false;
+  }
+  const size_t off = (size_t)T.uploaded[dev] * kPolyWords;
+  const size_t words = (size_t)need * kPolyWords - off;
+  if (cudaMemcpyToSymbolAsync(g_jump_poly, T.polys.data() + off, words * sizeof(uint64_t), off * sizeof(uint64_t),
+                              cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  T.uploaded[dev] = need;
+  return true;
+}
+
+// Segments of x_1248 .. x_{total-1}; 1 means one CTA generates the whole stream.
+static int segments(int64_t total) {
+  if (total < kWinEnd + kSeg) return 1;
+  const int64_t s = ceil_div(total - 2 * kN, kSeg);
+  return (int)(s < kMaxJumps + 1 ? s : kMaxJumps + 1);  // the last segment runs to the end
+}
+
 struct Plan {
   int64_t Wi, Aw, n_gen, nbI, nbA;
+  int nseg;
   size_t bytes;
   Scalars* sc;
   uint32_t* backup;  // the incoming state, for the gated walk
   uint32_t* raw;
+  uint32_t* part;    // (nseg - 1, kJumpParts, 624) partial start words of the segments
   int32_t* cnt_i;
   int32_t* cnt_a;
 };
@@ -501,6 +794,8 @@ static Plan plan(void* ws, int64_t count, uint32_t rng, uint32_t mask, int64_t G
   p.sc = c.take<Scalars>(1);
   p.backup = c.take<uint32_t>(kN + 4);
   p.raw = c.take<uint32_t>((size_t)(p.n_gen + 1) * kN);
+  p.nseg = segments((p.n_gen + 1) * kN);
+  p.part = c.take<uint32_t>((size_t)(p.nseg - 1) * kJumpParts * kN);
   p.cnt_i = c.take<int32_t>((size_t)p.nbI + 1);
   p.cnt_a = c.take<int32_t>((size_t)p.nbA + 1);
   p.bytes = c.bytes();
@@ -513,21 +808,29 @@ static int run_parallel(const Plan& p, uint32_t* state, int64_t count, int k, ui
   UMAPB_CUDA_TRY(cudaMemcpyAsync(p.backup, state, (kN + 4) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream),
                  "random draws: state copy");
   int launches = 3;
-  stream_kernel<<<1, kStreamThreads, 0, stream>>>(state, (p.n_gen + 1) * kN, p.raw);
+  const int64_t total = (p.n_gen + 1) * kN;
+  if (p.nseg > 1 && jump_table_ready(p.nseg - 1, stream)) {
+    stream_kernel<<<1, kStreamThreads, 0, stream>>>(state, kWinEnd, p.raw);
+    jump_kernel<<<(unsigned)((p.nseg - 1) * kJumpParts), kJumpThreads, 0, stream>>>(p.raw, p.part);
+    segment_kernel<<<(unsigned)p.nseg, kStreamThreads, 0, stream>>>(p.part, total, p.nseg, p.raw);
+    launches += 2;
+  } else {
+    stream_kernel<<<1, kStreamThreads, 0, stream>>>(state, total, p.raw);
+  }
   if (count > 0 && rng == 0) {
     const int64_t want = (count + 255) / 256;
     const_ints_kernel<<<(unsigned)(want < 4096 ? want : 4096), 256, 0, stream>>>(count, k, idx);
     ++launches;
   } else if (count > 0) {
     int_count_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i);
-    scan_exclusive_kernel<<<1, 1024, 0, stream>>>(p.cnt_i, p.nbI, &p.sc->tot_int);
+    scan_exclusive(p.cnt_i, p.nbI, &p.sc->tot_int, stream);
     int_scatter_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i, count, k, idx,
                                                              p.sc);
     launches += 3;
   }
   if (G > 0) {
     att_count_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a);
-    scan_exclusive_kernel<<<1, 1024, 0, stream>>>(p.cnt_a, p.nbA, &p.sc->tot_att);
+    scan_exclusive(p.cnt_a, p.nbA, &p.sc->tot_att, stream);
     att_scatter_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a, G, out);
     launches += 3;
   }
@@ -627,5 +930,18 @@ extern "C" int umapb_legacy_normal(uint32_t* state, int64_t count, double loc, d
   rstart::walk_kernel<<<1, rstart::kThreads, 0, stream>>>(state, state, nullptr, 1, 0, 1u, 1u, nullptr, count, o);
   UMAPB_LAUNCH_CHECK("legacy_normal kernel");
   count_launches(1);
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_mt_jump_poly(int32_t b, uint64_t* out, int64_t* words_ahead) {
+  clear_error();
+  UMAPB_REQUIRE(out && b >= 1 && b <= rstart::kMaxJumps, "mt_jump_poly: need 1 <= b <= %d and an output",
+                rstart::kMaxJumps);
+  rstart::jumps::Table& T = rstart::jumps::table();
+  std::lock_guard<std::mutex> lock(T.mu);
+  if (!rstart::jumps::extend(T, b))
+    return set_error(UMAPB_ERR_UNSUPPORTED, "mt_jump_poly: the characteristic polynomial was not found");
+  for (int q = 0; q < rstart::kPolyWords; ++q) out[q] = T.polys[(size_t)(b - 1) * rstart::kPolyWords + q];
+  if (words_ahead) *words_ahead = (int64_t)b * rstart::kSeg;
   return UMAPB_OK;
 }

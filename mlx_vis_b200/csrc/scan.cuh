@@ -1,44 +1,86 @@
-// Single-block exclusive scan used by the order-preserving compactions.
+// Exclusive scan used by the order-preserving compactions.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace umapb {
 
-// Exclusive scan of `count` int32 values in place by ONE block of 1024 threads;
-// writes the grand total to *total.  Each pass covers 1024 x 16 values (one pass
-// for up to 16 K values, five for 70 K): a thread scans its 16 consecutive values
-// in registers (four 16-byte loads), the block scans the thread sums (warp
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 16;                              // values per thread and pass
+constexpr int64_t kScanPass = (int64_t)kScanThreads * kScanItems;  // 16 K values per pass
+constexpr int kScanMaxBlocks = 64;
+
+// Blocks and values per block of a scan of `count` values: ranges of at least one
+// pass (16 K values), at most kScanMaxBlocks of them, each a multiple of 16 values so
+// that every range starts on a 16-byte boundary when the array does.
+inline void scan_shape(int64_t count, int* blocks, int64_t* span) {
+  int64_t b = (count + kScanPass - 1) / kScanPass;
+  if (b < 1) b = 1;
+  if (b > kScanMaxBlocks) b = kScanMaxBlocks;
+  int64_t s = (count + b - 1) / b;
+  s = (s + 15) / 16 * 16;
+  if (s < 16) s = 16;
+  *blocks = (int)((count + s - 1) / s > 0 ? (count + s - 1) / s : 1);
+  *span = s;
+}
+
+// Exclusive scan of `count` int32 values in place, in ONE launch without any wait
+// between blocks: block b owns [b span, (b + 1) span) and first sums every value
+// before its range itself (16-byte loads, all in flight at once; at most
+// kScanMaxBlocks / 2 times the array is read again, from L2 at the sizes the
+// pipeline scans), then scans its range in passes of 16 K values: a thread scans its
+// 16 consecutive values in registers, the block scans the thread sums (warp
 // shuffles, then one warp over the 32 warp sums) and a running carry links the
-// passes.
+// passes.  The last block writes the grand total to *total.
 template <int kDummy = 0>
-__global__ void __launch_bounds__(1024) scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
-                                                              int64_t* __restrict__ total) {
-  constexpr int kItems = 16;
+__global__ void __launch_bounds__(kScanThreads) scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
+                                                                      int64_t span, int64_t* __restrict__ total) {
   __shared__ int64_t warp_sums[32];
   __shared__ int64_t carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t span = (int64_t)blockDim.x * kItems;
   const bool aligned = (reinterpret_cast<uintptr_t>(vals) & 15) == 0;
-  for (int64_t base = 0; base < count; base += span) {
-    const int64_t first = base + (int64_t)threadIdx.x * kItems;
-    int32_t v[kItems];
-    const bool full = aligned && first + kItems <= count;
+  const int64_t lo = (int64_t)blockIdx.x * span;
+  const int64_t hi = lo + span < count ? lo + span : count;
+
+  // the sum of vals[0, lo)
+  int64_t pre = 0;
+  if (aligned) {
+    for (int64_t i = 4 * (int64_t)threadIdx.x; i < lo; i += 4 * (int64_t)kScanThreads) {
+      const int4 a = *reinterpret_cast<const int4*>(vals + i);  // lo is a multiple of 16
+      pre += (int64_t)a.x + a.y + a.z + a.w;
+    }
+  } else {
+    for (int64_t i = threadIdx.x; i < lo; i += kScanThreads) pre += vals[i];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
+  if (lane == 0) warp_sums[warp] = pre;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t s = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) s += warp_sums[w];
+    carry = s;
+  }
+  __syncthreads();
+
+  for (int64_t base = lo; base < hi; base += kScanPass) {
+    const int64_t first = base + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems];
+    const bool full = aligned && first + kScanItems <= hi;
     if (full) {
 #pragma unroll
-      for (int q = 0; q < kItems / 4; ++q) {
+      for (int q = 0; q < kScanItems / 4; ++q) {
         const int4 a = *reinterpret_cast<const int4*>(vals + first + 4 * q);
         v[4 * q] = a.x, v[4 * q + 1] = a.y, v[4 * q + 2] = a.z, v[4 * q + 3] = a.w;
       }
     } else {
 #pragma unroll
-      for (int u = 0; u < kItems; ++u) v[u] = first + u < count ? vals[first + u] : 0;
+      for (int u = 0; u < kScanItems; ++u) v[u] = first + u < hi ? vals[first + u] : 0;
     }
     int64_t sum = 0;
 #pragma unroll
-    for (int u = 0; u < kItems; ++u) sum += v[u];
+    for (int u = 0; u < kScanItems; ++u) sum += v[u];
     int64_t x = sum;  // inclusive scan of the thread sums within the warp
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -48,7 +90,7 @@ __global__ void __launch_bounds__(1024) scan_exclusive_kernel(int32_t* __restric
     if (lane == 31) warp_sums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-      int64_t s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+      int64_t s = warp_sums[lane];
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
@@ -59,25 +101,33 @@ __global__ void __launch_bounds__(1024) scan_exclusive_kernel(int32_t* __restric
     __syncthreads();
     int64_t run = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + x - sum;
 #pragma unroll
-    for (int u = 0; u < kItems; ++u) {  // exclusive prefix, in place
+    for (int u = 0; u < kScanItems; ++u) {  // exclusive prefix, in place
       const int32_t t = v[u];
       v[u] = (int32_t)run;
       run += t;
     }
     if (full) {
 #pragma unroll
-      for (int q = 0; q < kItems / 4; ++q)
+      for (int q = 0; q < kScanItems / 4; ++q)
         *reinterpret_cast<int4*>(vals + first + 4 * q) = make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
     } else {
 #pragma unroll
-      for (int u = 0; u < kItems; ++u)
-        if (first + u < count) vals[first + u] = v[u];
+      for (int u = 0; u < kScanItems; ++u)
+        if (first + u < hi) vals[first + u] = v[u];
     }
     __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = run;
+    if (threadIdx.x == kScanThreads - 1) carry = run;
     __syncthreads();
   }
-  if (threadIdx.x == 0) *total = carry;
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total = carry;
+}
+
+// Enqueue the scan of vals[0, count) (count >= 0) on `stream`.
+inline void scan_exclusive(int32_t* vals, int64_t count, int64_t* total, cudaStream_t stream) {
+  int blocks;
+  int64_t span;
+  scan_shape(count, &blocks, &span);
+  scan_exclusive_kernel<<<blocks, kScanThreads, 0, stream>>>(vals, count, span, total);
 }
 
 }  // namespace umapb

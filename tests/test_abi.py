@@ -77,3 +77,43 @@ def test_python_signatures_have_the_header_arity():
         params = params.strip()
         n = 0 if params in ("", "void") else params.count(",") + 1
         assert len(_lib.SIGNATURES[name]) == n, (name, n, len(_lib.SIGNATURES[name]))
+
+
+def _raw_words(key, total):
+    """x_0..x_{total-1}: the key, then x_n = x_{n-227} ^ mix(x_{n-624}, x_{n-623})."""
+    import numpy as np
+
+    x = np.zeros(total, dtype=np.uint32)
+    x[:624] = key
+    for base in range(624, total, 227):
+        n = np.arange(base, min(total, base + 227))
+        y = (x[n - 624] & np.uint32(0x80000000)) | (x[n - 623] & np.uint32(0x7FFFFFFF))
+        x[n] = x[n - 227] ^ (y >> np.uint32(1)) ^ np.where(y & np.uint32(1), np.uint32(0x9908B0DF), np.uint32(0))
+    return x
+
+
+def test_mt_jump_polynomials_step_the_raw_stream(lib):
+    """umapb_mt_jump_poly (host code): the words D = b * 65536 ahead of any position
+    n >= 1 are the XOR of the words at n + i over the polynomial's set exponents i --
+    the identity the device segments start from."""
+    import numpy as np
+
+    from mlx_vis_b200 import _lib
+    from oracle.mt19937 import twist
+
+    key = np.random.RandomState(11).get_state()[1]
+    x = _raw_words(key, 5 * 65536 + 1300)
+    g = [int(v) for v in key]
+    for gen in range(1, 4):  # the vectorised recurrence is the published twist
+        g = twist(g)
+        assert np.array_equal(x[624 * gen:624 * (gen + 1)], np.array(g, dtype=np.uint32))
+    w = np.arange(624)
+    for b, base in ((1, 1), (1, 624), (2, 700), (5, 624)):
+        bits, D = _lib.mt_jump_poly(b)
+        assert D == b * 65536 and bits.sum() > 1000
+        e = np.nonzero(bits)[0]
+        got = np.bitwise_xor.reduce(x[base + e[:, None] + w[None, :]], axis=0)
+        assert np.array_equal(got, x[base + D + w])
+    for bad in (0, 1025):
+        with pytest.raises(_lib.UmapB200Error):
+            _lib.mt_jump_poly(bad)

@@ -58,8 +58,10 @@ def test_split3_transpose_and_mean_with_k_slices():
     assert np.abs(cov - ref).max() < 1e-4 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("n", [1, 5, 1023, 1024, 1025, 70000])
+@pytest.mark.parametrize("n", [1, 5, 1023, 1024, 1025, 70000, 5_000_003])
 def test_sort_keys_is_a_stable_argsort(n):
+    """Also covers the exclusive scan of the tile histograms: 256 x tiles counts, one
+    block up to 16 K of them, several blocks (with several passes each) above."""
     from mlx_vis_b200 import _lib
 
     rng = np.random.default_rng(n)
