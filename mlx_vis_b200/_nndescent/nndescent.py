@@ -187,8 +187,9 @@ class NNDescent:
         dist2 = torch.empty_like(dist)
         flags = torch.ones((n, k), dtype=torch.uint8, device=dev)
         flags2 = torch.empty_like(flags)
-        changed = torch.zeros(1, dtype=torch.int64, device=dev)
-        evals = torch.zeros(1, dtype=torch.int64, device=dev)
+        # (changed, evals) counters of every iteration, zeroed once: an iteration
+        # launches no fill and the host reads both with one copy
+        counters = torch.zeros((max(self.n_iters, 1), 2), dtype=torch.int64, device=dev)
         Xh = None
         # blocked nn-of-nn join (full path); UMAPB_NND_JOIN=0 computes every
         # candidate distance inside the row kernel instead
@@ -202,8 +203,7 @@ class NNDescent:
         for it in range(self.n_iters):
             mc_nn, j_nn, mc_conv = iteration_params(update_frac, k, mc)
             use_rev = update_frac >= 0.10
-            changed.zero_()
-            evals.zero_()
+            changed, evals = counters[it, 0:1], counters[it, 1:2]
             ev = self._events()
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
@@ -265,12 +265,12 @@ class NNDescent:
                     call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx2), ptr(dist2), k, 0, s)
                 info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd,
                             elem=2 if use_half else 4, join=join)
-            n_changed = int(changed.item())  # the one host read per iteration
+            n_changed, n_evals = counters[it].tolist()  # the one host read per iteration
             update_frac = n_changed / (n * k)
             idx, idx2 = idx2, idx
             dist, dist2 = dist2, dist
             flags, flags2 = flags2, flags
-            info.update(it=it, changed=n_changed, evals=int(evals.item()), n=n, k=k,
+            info.update(it=it, changed=n_changed, evals=n_evals, n=n, k=k,
                         candidates=k + info["mc_new"] * j_nn + (k if use_rev else 0))
             if ev:
                 self.kernel_log_.append((ev[0], ev[1], info))

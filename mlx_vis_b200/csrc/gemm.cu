@@ -55,20 +55,10 @@ struct EpiArgs {
 };
 
 
-// Split-precision products (NPAIR = 6): A and B hold three BF16 parts per value,
-// x = x0 + x1 + x2 (x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1)),
-// side by side at column offsets 0, kp and 2 kp of each row.  The K loop then runs
-// over (K block, part pair) with the pairs (0,0) (0,1) (1,0) (0,2) (2,0) (1,1),
-// every product accumulated in the same FP32 TMEM tile: the dropped terms are
-// below 2^-24 of |a||b|, so C carries FP32-level error.  Consecutive iterations
-// reuse the K block's A and B tiles from L2.
-__constant__ int8_t kPairA[6] = {0, 0, 1, 0, 2, 1};
-__constant__ int8_t kPairB[6] = {0, 1, 0, 2, 0, 1};
-
-template <int EPI, int NPAIR = 1>
+template <int EPI>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int num_kb,
-                EpiArgs e, int32_t* __restrict__ status, int kp = 0, int n_major = 0) {
+                EpiArgs e, int32_t* __restrict__ status) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
@@ -78,14 +68,11 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // n_major: blockIdx.x walks the N tiles, so CTAs launched together share an A tile in L2
-  const int m0 = (n_major ? blockIdx.y : blockIdx.x) * BM, n0 = (n_major ? blockIdx.x : blockIdx.y) * BN;
-  // this CTA's K iterations [kb0, kb1) (K blocks x part pairs); the host sizes the
-  // slices so none is empty
-  const int num_it = num_kb * NPAIR;
-  const int per = (num_it + gridDim.z - 1) / gridDim.z;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  // this CTA's K blocks [kb0, kb1); the host sizes the slices so none is empty
+  const int per = (num_kb + gridDim.z - 1) / gridDim.z;
   const int kb0 = blockIdx.z * per;
-  const int kb1 = kb0 + per < num_it ? kb0 + per : num_it;
+  const int kb1 = kb0 + per < num_kb ? kb0 + per : num_kb;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -115,14 +102,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (!tc::mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
         uint8_t* sa = smem + s * STAGE_BYTES;
         tc::mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
-        int xa = kb * BK, xb = kb * BK;
-        if (NPAIR > 1) {
-          const int k = kb / NPAIR, pr = kb - k * NPAIR;
-          xa = kPairA[pr] * kp + k * BK;
-          xb = kPairB[pr] * kp + k * BK;
-        }
-        tc::tma_load_2d(sa, &tmA, &full[s], xa, m0);
-        tc::tma_load_2d(sa + A_BYTES, &tmB, &full[s], xb, n0);
+        tc::tma_load_2d(sa, &tmA, &full[s], kb * BK, m0);
+        tc::tma_load_2d(sa + A_BYTES, &tmB, &full[s], kb * BK, n0);
       }
     }
   } else if (warp == 1) {
@@ -217,6 +198,133 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (threadIdx.x == 0 && *abort_flag) atomicExch(status, (int32_t)kDevTimeoutEpilogue);
 }
 
+// Split-precision products: A and B hold three BF16 parts per value,
+// x = x0 + x1 + x2 (x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1)), side
+// by side at column offsets 0, kp and 2 kp of each row.  A stage holds all six part
+// tiles of one 64-wide K block (A0 A1 A2 B0 B1 B2, 96 KB; two stages), loaded once,
+// and the MMA thread issues the pairs (0,0) (0,1) (1,0) (0,2) (2,0) (1,1) from them
+// into one FP32 TMEM tile: the dropped terms are below 2^-24 of |a||b|, so C carries
+// FP32-level error.  K slices (gridDim.z) cut the K blocks; the F32 epilogue writes
+// slice z at C + z * slice.
+constexpr int S3_TILE = BM * BK * 2;              // one 128 x 64 BF16 part tile (BM == BN)
+constexpr int S3_STAGES = 2;
+constexpr int S3_STAGE_BYTES = 6 * S3_TILE;
+constexpr int S3_SMEM = 1024 + S3_STAGES * S3_STAGE_BYTES + 256;
+static_assert(BM == BN, "the split kernel's part tiles share one size");
+
+__global__ void __launch_bounds__(THREADS, 1)
+    split3_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int num_kb,
+                  EpiArgs e, int32_t* __restrict__ status, int kp) {
+  constexpr int kPa[6] = {0, 0, 1, 0, 2, 1};
+  constexpr int kPb[6] = {0, 1, 0, 2, 0, 1};
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S3_STAGES * S3_STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + S3_STAGES;
+  uint64_t* done = bars + 2 * S3_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // blockIdx.x walks the N tiles, so CTAs launched together share an A tile in L2
+  const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+  const int per = (num_kb + gridDim.z - 1) / gridDim.z;  // the host sizes the slices so none is empty
+  const int kb0 = blockIdx.z * per;
+  const int kb1 = kb0 + per < num_kb ? kb0 + per : num_kb;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S3_STAGES; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(done, 1);
+    *abort_flag = 0;
+    tc::fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    tc::prefetch_tmap(&tmA);
+    tc::prefetch_tmap(&tmB);
+  }
+  if (warp == 2) tc::tmem_alloc(tmem_slot, BN);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = kb0; kb < kb1; ++kb) {
+        const int i = kb - kb0;
+        const int s = i % S3_STAGES;
+        const uint32_t ph = (uint32_t)(i / S3_STAGES) & 1u;
+        if (!tc::mbar_wait(&empty[s], ph ^ 1u, abort_flag)) break;
+        uint8_t* st = smem + s * S3_STAGE_BYTES;
+        tc::mbar_arrive_expect_tx(&full[s], S3_STAGE_BYTES);
+#pragma unroll
+        for (int p = 0; p < 3; ++p) {
+          tc::tma_load_2d(st + p * S3_TILE, &tmA, &full[s], p * kp + kb * BK, m0);
+          tc::tma_load_2d(st + (3 + p) * S3_TILE, &tmB, &full[s], p * kp + kb * BK, n0);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(BM, BN);
+      bool ok = true;
+      for (int kb = kb0; kb < kb1; ++kb) {
+        const int i = kb - kb0;
+        const int s = i % S3_STAGES;
+        const uint32_t ph = (uint32_t)(i / S3_STAGES) & 1u;
+        if (!tc::mbar_wait(&full[s], ph, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t st = tc::smem_u32(smem + s * S3_STAGE_BYTES);
+#pragma unroll
+        for (int pr = 0; pr < 6; ++pr) {
+          const uint32_t a_addr = st + kPa[pr] * S3_TILE, b_addr = st + (3 + kPb[pr]) * S3_TILE;
+#pragma unroll
+          for (int k = 0; k < BK / UK; ++k)
+            tc::mma_bf16(tmem_base, tc::sw128_kmajor_desc(a_addr + k * 32), tc::sw128_kmajor_desc(b_addr + k * 32),
+                         idesc, (i | pr | k) != 0 ? 1u : 0u);
+        }
+        tc::mma_commit(&empty[s]);
+      }
+      if (ok) tc::mma_commit(done);
+    }
+  } else {
+    // epilogue: thread = accumulator row (TMEM lane), 32 columns per tcgen05.ld,
+    // staged through this warp's 32 x 33 float tile in the drained stage memory so a
+    // warp instruction writes 32 consecutive columns of one row
+    const int q = warp & 3;
+    const int rbase = m0 + q * 32;
+    float* S = reinterpret_cast<float*>(smem) + q * 32 * 33;
+    if (tc::mbar_wait(done, 0, abort_flag)) {
+      tc::tc_fence_after();
+      float* C = e.C + blockIdx.z * e.slice;
+      for (int ch = 0; ch < BN / 32 && n0 + ch * 32 < e.N; ++ch) {
+        float v[32];
+        __syncwarp();
+        tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(ch * 32), v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) S[lane * 33 + j] = v[j];
+        __syncwarp();
+        const int n = n0 + ch * 32 + lane;
+        if (n < e.N)
+          for (int rr = 0; rr < 32 && rbase + rr < e.M; ++rr) C[(int64_t)(rbase + rr) * e.ldc + n] = S[rr * 33 + lane];
+      }
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem_base, BN);
+  }
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(status, (int32_t)kDevTimeoutEpilogue);
+}
+
 template <int EPI>
 static int launch(const void* A, const void* B, int M, int N, int K, int lda, int ldb, int ksplit, const EpiArgs& e,
                   int32_t* status, cudaStream_t stream) {
@@ -297,8 +405,8 @@ extern "C" int umapb_gemm_split3(const void* A3, const void* B3, int32_t M, int3
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && !attr[dev]) {
-    UMAPB_CUDA_TRY(cudaFuncSetAttribute(gemm::gemm_kernel<gemm::EPI_F32, 6>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, gemm::SMEM),
+    UMAPB_CUDA_TRY(cudaFuncSetAttribute(gemm::split3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        gemm::S3_SMEM),
                    "gemm_split3: smem attribute");
     attr[dev] = true;
   }
@@ -308,16 +416,15 @@ extern "C" int umapb_gemm_split3(const void* A3, const void* B3, int32_t M, int3
   if ((s = make_tmap_bf16_2d(&ta, A3, (uint64_t)M, w, w, gemm::BM, gemm::BK))) return s;
   if ((s = make_tmap_bf16_2d(&tb, B3, (uint64_t)N, w, w, gemm::BN, gemm::BK))) return s;
   const int num_kb = kp / gemm::BK;
-  const int num_it = num_kb * 6;
-  const int per = (int)ceil_div(num_it, ksplit);
-  const int slices = (int)ceil_div(num_it, per);
+  const int per = (int)ceil_div(num_kb, ksplit);
+  const int slices = (int)ceil_div(num_kb, per);  // every slice gets at least one K block
   gemm::EpiArgs e{M, N, C, ldc, nullptr, nullptr, 0, nullptr, 0, nullptr, 0, nullptr, (int64_t)M * ldc};
-  if (slices < ksplit)
+  if (slices < ksplit)  // the caller sums ksplit slices: the ones without K blocks hold zeros
     UMAPB_CUDA_TRY(cudaMemsetAsync(C + slices * e.slice, 0, sizeof(float) * (size_t)(ksplit - slices) * e.slice,
                                    stream),
                    "gemm_split3: empty slices");
   dim3 grid((unsigned)ceil_div(N, gemm::BN), (unsigned)ceil_div(M, gemm::BM), (unsigned)slices);
-  gemm::gemm_kernel<gemm::EPI_F32, 6><<<grid, gemm::THREADS, gemm::SMEM, stream>>>(ta, tb, num_kb, e, status, kp, 1);
+  gemm::split3_kernel<<<grid, gemm::THREADS, gemm::S3_SMEM, stream>>>(ta, tb, num_kb, e, status, kp);
   UMAPB_LAUNCH_CHECK("gemm_split3 kernel launch");
   count_launches(1);
   return UMAPB_OK;

@@ -51,21 +51,41 @@ __device__ __forceinline__ void split_value(float x, __nv_bfloat16& b0, __nv_bfl
   b2 = __float2bfloat16_rn(r2);
 }
 
-// operand row r = stored row r; columns c < cols hold S[r][c] - mu[c], [cols, kp) zeros
+// operand row r = stored row r; columns c < cols hold S[r][c] - mu[c], [cols, kp) zeros.
+// A thread splits 8 consecutive columns: two 16-byte loads (when S's rows and mu are
+// 16-byte aligned and the group lies inside the row) and one 16-byte store per part.
 __global__ void split_rows_kernel(const float* __restrict__ S, int64_t rows, int64_t cols, int64_t lds,
-                                  const float* __restrict__ mu, int kp, __nv_bfloat16* __restrict__ out) {
+                                  const float* __restrict__ mu, int kp, int vec, __nv_bfloat16* __restrict__ out) {
+  const int groups = kp / 8;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t r = t / kp;
-  const int c = (int)(t - r * kp);
+  const int64_t r = t / groups;
+  const int c0 = (int)(t - r * groups) * 8;
   if (r >= rows) return;
-  float x = 0.f;
-  if (c < cols) x = mu ? __fsub_rn(S[r * lds + c], mu[c]) : S[r * lds + c];
-  __nv_bfloat16 b0, b1, b2;
-  split_value(x, b0, b1, b2);
-  __nv_bfloat16* o = out + r * 3 * (int64_t)kp;
-  o[c] = b0;
-  o[kp + c] = b1;
-  o[2 * kp + c] = b2;
+  float x[8];
+  const float* src = S + r * lds + c0;
+  if (vec && c0 + 8 <= cols) {
+    const float4 a = *reinterpret_cast<const float4*>(src), b = *reinterpret_cast<const float4*>(src + 4);
+    x[0] = a.x, x[1] = a.y, x[2] = a.z, x[3] = a.w, x[4] = b.x, x[5] = b.y, x[6] = b.z, x[7] = b.w;
+    if (mu) {
+      const float4 ma = *reinterpret_cast<const float4*>(mu + c0), mb = *reinterpret_cast<const float4*>(mu + c0 + 4);
+      const float m[8] = {ma.x, ma.y, ma.z, ma.w, mb.x, mb.y, mb.z, mb.w};
+#pragma unroll
+      for (int u = 0; u < 8; ++u) x[u] = __fsub_rn(x[u], m[u]);
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int c = c0 + u;
+      x[u] = c < cols ? (mu ? __fsub_rn(src[u], mu[c]) : src[u]) : 0.f;
+    }
+  }
+  __align__(16) __nv_bfloat16 p0[8], p1[8], p2[8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u) split_value(x[u], p0[u], p1[u], p2[u]);
+  uint4* o = reinterpret_cast<uint4*>(out + r * 3 * (int64_t)kp + c0);  // kp % 8 == 0: 16-byte aligned
+  o[0] = *reinterpret_cast<const uint4*>(p0);
+  o[kp / 8] = *reinterpret_cast<const uint4*>(p1);
+  o[kp / 4] = *reinterpret_cast<const uint4*>(p2);
 }
 
 // operand row c = stored column c; columns r < rows hold S[r][c] - mu[c], [rows, kp)
@@ -224,8 +244,11 @@ extern "C" int umapb_split3(const float* S, int64_t rows, int64_t cols, int64_t 
   UMAPB_REQUIRE(kp >= (transpose ? rows : cols), "split3: kp must cover the operand's K extent");
   __nv_bfloat16* o = static_cast<__nv_bfloat16*>(out);
   if (!transpose) {
-    const int64_t total = rows * kp;
-    linalg::split_rows_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(S, rows, cols, lds, mu, kp, o);
+    const int64_t total = rows * (kp / 8);
+    const int vec = (reinterpret_cast<uintptr_t>(S) & 15) == 0 && lds % 4 == 0 &&
+                    (!mu || (reinterpret_cast<uintptr_t>(mu) & 15) == 0);
+    linalg::split_rows_kernel<<<(unsigned)ceil_div(total, 256), 256, 0, stream>>>(S, rows, cols, lds, mu, kp, vec,
+                                                                                   o);
   } else {
     UMAPB_REQUIRE(ceil_div(cols, 32) < 65536, "split3: too many columns to transpose");
     linalg::split_cols_kernel<<<dim3((unsigned)ceil_div(kp, 32), (unsigned)ceil_div(cols, 32)), dim3(32, 8), 0,
