@@ -95,6 +95,39 @@ __device__ __forceinline__ float d2_from_dot(float sq_i, float sq_c, float dot, 
   return fmaxf(__fsub_rn(__fadd_rn(sq_i, sq_c), __fmul_rn(2.0f, dot)), 0.0f);
 }
 
+// ascending bitonic sort of one (distance, id) key per lane across the warp
+__device__ __forceinline__ void warp_sort_keys(float& d, int& id, int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const float od = __shfl_xor_sync(0xffffffffu, d, stride);
+      const int oi = __shfl_xor_sync(0xffffffffu, id, stride);
+      const bool lower = (lane & stride) == 0, asc = (lane & size) == 0;
+      const bool take = (lower == asc) ? key_lt(od, oi, d, id) : key_lt(d, id, od, oi);
+      if (take) {
+        d = od;
+        id = oi;
+      }
+    }
+  }
+}
+
+// ascending order of a bitonic sequence held one key per lane
+__device__ __forceinline__ void warp_bitonic_clean(float& d, int& id, int lane) {
+#pragma unroll
+  for (int stride = 16; stride > 0; stride >>= 1) {
+    const float od = __shfl_xor_sync(0xffffffffu, d, stride);
+    const int oi = __shfl_xor_sync(0xffffffffu, id, stride);
+    const bool take = (lane & stride) == 0 ? key_lt(od, oi, d, id) : key_lt(d, id, od, oi);
+    if (take) {
+      d = od;
+      id = oi;
+    }
+  }
+}
+
+// Inserts (d, id) into the warp-distributed ascending list (lane l holds entry l).
 // Inserts (d, id) into the warp-distributed ascending list (lane l holds entry l).
 __device__ __forceinline__ void list_insert(float& lv, int& li, float d, int id, int k, int lane) {
   const int pos = __popc(__ballot_sync(0xffffffffu, lane < k && key_lt(lv, li, d, id)));
@@ -166,21 +199,7 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, const float* __r
       }
     }
   }
-  if (sort_rows) {  // warp bitonic sort of k <= 32 (distance, id) pairs held one per lane
-    for (int size = 2; size <= 32; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const float od = __shfl_xor_sync(0xffffffffu, my_d, stride);
-        const int oi = __shfl_xor_sync(0xffffffffu, my_i, stride);
-        const bool lower = (lane & stride) == 0;
-        const bool asc = (lane & size) == 0;
-        const bool take_other = (lower == asc) ? key_lt(od, oi, my_d, my_i) : key_lt(my_d, my_i, od, oi);
-        if (take_other) {
-          my_d = od;
-          my_i = oi;
-        }
-      }
-    }
-  }
+  if (sort_rows) warp_sort_keys(my_d, my_i, lane);  // k <= 32 (distance, id) pairs, one per lane
   if (lane < k) {
     idx[row * k + lane] = my_i;
     dist[row * k + lane] = my_d;
@@ -739,18 +758,28 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   // 1. candidate ids in the reference's column order
   const int nn_cols = a.mc_new * a.j_nn;
   const int T_total = k + nn_cols + (a.rev ? k : 0);
-  for (int t = lane; t < a.tcap; t += 32) {
-    int id = 0x7fffffff;
-    if (t < k) {
-      id = orow[t];
-    } else if (t < k + nn_cols) {
-      const int q = t - k;
-      const int src = srcs[q / a.j_nn];
-      id = a.idx_old[(int64_t)src * k + (q % a.j_nn)];
-    } else if (t < T_total) {
-      id = a.rev[row * k + (t - k - nn_cols)];
+  // four chunks at a time: their loads are issued together, one round trip
+  for (int g0 = 0; g0 < a.tcap; g0 += 128) {
+    const int32_t* src_p[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = g0 + 32 * u + lane;
+      src_p[u] = nullptr;
+      if (t < k) {
+        src_p[u] = orow + t;
+      } else if (t < k + nn_cols) {
+        const int q = t - k;
+        src_p[u] = a.idx_old + (int64_t)srcs[q / a.j_nn] * k + (q % a.j_nn);
+      } else if (t < T_total) {
+        src_p[u] = a.rev + row * k + (t - k - nn_cols);
+      }
     }
-    cid[t] = id;
+    int v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v[u] = src_p[u] ? __ldg(src_p[u]) : 0x7fffffff;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (g0 + 32 * u < a.tcap) cid[g0 + 32 * u + lane] = v[u];
   }
   __syncwarp();
 
@@ -834,16 +863,43 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   }
   __syncwarp();
 
-  // 4. k smallest (distance, id) over all candidate columns
-  float lv = kBig * 4.0f;  // above every real key, including 1e30 entries
+  // 4. k smallest (distance, id) over all candidate columns.  The list sits one key
+  // per lane, ascending, sentinels past k.  Keys of a chunk below the current k-th are
+  // inserted one at a time (a ballot, two shuffles); a chunk with more than 10 of them
+  // (the first chunk, when the list is empty) is sorted across the warp (bitonic, 15
+  // exchange steps) and merged: the 32 smallest of the list and the sorted chunk,
+  // paired in reverse, form a bitonic sequence that five exchange steps order.
+  constexpr float kSent = kBig * 4.0f;  // above every real key, including 1e30 entries
+  float lv = kSent;
   int li = 0x7fffffff;
   float tau = lv;
   int tau_i = li;
   for (int t0 = 0; t0 < a.tcap; t0 += 32) {
     const int t = t0 + lane;
-    const float d = t < T_total ? cd[t] : INFINITY;
-    const int id = cid[t];
+    float d = t < T_total ? cd[t] : kSent;
+    int id = t < T_total ? cid[t] : 0x7fffffff;
     unsigned b = __ballot_sync(0xffffffffu, t < T_total && key_lt(d, id, tau, tau_i));
+    if (__popc(b) > 10) {
+      if (!((b >> lane) & 1u)) {
+        d = kSent;
+        id = 0x7fffffff;
+      }
+      warp_sort_keys(d, id, lane);
+      const float od = __shfl_sync(0xffffffffu, d, 31 - lane);
+      const int oi = __shfl_sync(0xffffffffu, id, 31 - lane);
+      if (key_lt(od, oi, lv, li)) {
+        lv = od;
+        li = oi;
+      }
+      warp_bitonic_clean(lv, li, lane);
+      if (lane >= k) {
+        lv = kSent;
+        li = 0x7fffffff;
+      }
+      tau = __shfl_sync(0xffffffffu, lv, k - 1);
+      tau_i = __shfl_sync(0xffffffffu, li, k - 1);
+      continue;
+    }
     while (b) {
       const int src = __ffs(b) - 1;
       const float sd = __shfl_sync(0xffffffffu, d, src);
