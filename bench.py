@@ -14,9 +14,12 @@ offline), NNDescent k=15 with the reference's defaults (n_iters 20, delta
   roofline  the layout epoch (sgd_epoch_kernel + apply_kernel), the largest
           kernel share of a fit: 112 algorithmic bytes per active edge over the
           layout stage's CUDA-event time divided by the epochs
+          (+ random_access: 8-byte random reads and atomic adds per second against
+          a probe of that access rate on the same table)
   roofline_nndescent  one NNDescent iteration (join + row kernel), CUDA events
           around each launch in the timed fits, against two byte counts: every
           reference candidate row read once, and the rows the blocked join reads
+          (+ row_gather: the rows' bytes at a probe's rate for random rows)
   knn_brute  the 20000 x 784 exact-kNN workload (untimed record): its three
           launches timed with CUDA events, tile kernel against the BF16 peak
   learned_init  layout epochs the learned warm start needs to reach the
@@ -225,6 +228,58 @@ def committed_traffic(name: str = "nnd_iteration_70k.md"):
 
 
 # --------------------------------------------------------------------------
+def _row_bytes(info) -> int:
+    """Bytes of one distance-space row of an NNDescent iteration (FP16 rows padded to
+    multiples of 8 elements)."""
+    if info["elem"] == 2:
+        return (info["space"] + 7) // 8 * 8 * 2
+    return info["space"] * 4
+
+
+def access_probes(torch, n, row_sizes):
+    """Measured ceilings of the two gather-bound steps (untimed, after the timed fits):
+    random 8-byte reads and atomic adds on an n x 2 table, 4 reads per add (the
+    layout's Y; an epoch makes 7 reads and 2 adds per active edge), and one warp per
+    random row of each distance-space row size (the NNDescent join's row reads,
+    31 n rows)."""
+    from mlx_vis_b200 import _lib
+
+    dev = torch.device("cuda")
+    s = _lib.stream_handle()
+
+    def best(fn, reps=5):
+        fn()
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) * 1e-3)
+        return min(ts)
+
+    table = torch.rand((n, 2), device=dev)
+    dtab = torch.zeros((n, 2), device=dev)
+    sink = torch.zeros(16, device=dev)
+    threads = torch.cuda.get_device_properties(dev).multi_processor_count * 2048
+    per, red = 128, 4
+    t = best(lambda: _lib.call("umapb_probe_random_access", _lib.ptr(table), _lib.ptr(dtab), n, 2, threads, per, red,
+                               _lib.ptr(sink), s))
+    random_rate = threads * (per + (per + red - 1) // red) / t
+    ids = torch.randint(0, n, (31 * n,), dtype=torch.int32, device=dev)
+    rates = {}
+    for rb in sorted(set(row_sizes)):
+        tab = torch.randint(0, 255, (n * rb,), dtype=torch.uint8, device=dev)
+        t = best(lambda: _lib.call("umapb_probe_row_gather", _lib.ptr(tab), n, rb, _lib.ptr(ids), ids.numel(),
+                                   _lib.ptr(sink), s))
+        rates[rb] = ids.numel() * rb / t
+        del tab
+    return random_rate, rates
+
+
 def max_over_ranks(value: float, dist, device) -> float:
     """The largest per-rank value (a time): every rank calls this at the same point."""
     if dist is None:
@@ -363,6 +418,32 @@ def run_ours(args, rank, world, local_rank):
                     "note": "reference bytes count every row of the reference's candidate list as read once "
                             "(above the HBM rate because the join reuses rows); blocked bytes are the rows the "
                             "join and the row kernel must read"}
+
+    # measured ceilings of the two gather-bound steps (rank 0, untimed)
+    if rank == 0:
+        last = models[-1].nndescent_.kernel_log_
+        sizes = [_row_bytes(info) for _, _, info in last]
+        random_rate, row_rates = access_probes(torch, n, sizes)
+        acc_epoch = 9.0 * edges_per_fit / N_EPOCHS  # 7 reads + 2 atomic adds per active edge (rate 5, 2-D)
+        roofline["random_access"] = {
+            "achieved_g_per_s": round(acc_epoch / t_epoch / 1e9, 1), "probe_g_per_s": round(random_rate / 1e9, 1),
+            "frac": round(acc_epoch / t_epoch / random_rate, 3),
+            "note": "8-byte random reads and atomic adds per second; the probe "
+                    "(umapb_probe_random_access) makes 4 random reads per atomic add on the same n x 2 table, "
+                    "the epoch 7 reads and 2 adds per active edge"}
+        bound = 0.0
+        for (e0, e1, info), rb in zip(last, sizes):
+            rows = info["n"] * (info["mc_new"] + 1 + info["j_nn"] if info.get("join") else
+                                info["candidates"] - info["k"] + 1)
+            bound += rows * rb / row_rates[rb]
+        meas = sum(e0.elapsed_time(e1) for e0, e1, _ in last) * 1e-3
+        roofline_nnd["row_gather"] = {
+            "probe_gb_per_s": {str(rb): round(r / 1e9, 1) for rb, r in row_rates.items()},
+            "bound_ms_per_fit": round(bound * 1e3, 3), "measured_ms_per_fit": round(meas * 1e3, 3),
+            "frac": round(bound / meas, 3),
+            "note": "bound: each iteration's candidate-row bytes (the join's rows, or the reference's candidate "
+                    "rows when the row kernel computes every distance) at the probe's rate for random rows of that "
+                    "size (umapb_probe_row_gather, one warp per row)"}
 
     # ---- end to end through the public API (pinned host input, host output) ----
     barrier()

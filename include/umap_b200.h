@@ -60,7 +60,10 @@ int umapb_set_wait_limit_ns(unsigned long long ns);
  *   X        (n, d) float32
  *   out_idx  (n, k) int32   ascending distance, self excluded
  *   out_dist (n, k) float32 Euclidean (squared != 0: squared distances)
- * Requires 1 <= k <= n-1 and k + extra <= 128.
+ * Requires 1 <= k <= n-1.  Lists of k + extra <= 128 candidates come from the
+ * fused tiles and the rerank; longer ones (k <= 4096) from exact FP32-level
+ * distance tiles (the split-precision GEMM) and a per-row radix select, which
+ * uses no candidates (extra is ignored there; umapb_knn_brute_timed refuses them).
  * ------------------------------------------------------------------------- */
 int umapb_knn_brute_workspace(int64_t n, int64_t d, int32_t k, int32_t extra, size_t* bytes);
 int umapb_knn_brute(const float* X, int64_t n, int64_t d, int32_t k, int32_t extra, int32_t squared,
@@ -387,6 +390,23 @@ int umapb_sort_keys_workspace(int64_t n, size_t* bytes);
 int umapb_sort_keys(const float* keys, int64_t n, int64_t stride, int32_t* order, void* workspace,
                     size_t workspace_bytes,
                     umapb_stream_t stream);
+
+/* ---------------------------------------------------------------------------
+ * Access-rate probes (measurement; no reference counterpart).  The caller times one
+ * launch; they give the measured ceilings the two gather-bound steps are reported
+ * against.
+ * umapb_probe_random_access: threads (a multiple of 256) x per_thread rounds of one
+ *   random row read of dim floats (dim 1, 2 or 4) from table (n rows) and, every
+ *   red_every rounds (0: never), one random vector atomic add of dim floats into
+ *   dtable -- the access mix of a layout epoch.  sink: 4 device floats.
+ * umapb_probe_row_gather: one warp per entry of ids reads the row of row_bytes (a
+ *   multiple of 16, 16-byte aligned table) -- the candidate-row reads of the
+ *   NNDescent join.  Ids outside [0, rows) are skipped.  sink: 16 device bytes.
+ * ------------------------------------------------------------------------- */
+int umapb_probe_random_access(const float* table, float* dtable, int64_t n, int32_t dim, int64_t threads,
+                              int32_t per_thread, int32_t red_every, float* sink, umapb_stream_t stream);
+int umapb_probe_row_gather(const void* table, int64_t rows, int32_t row_bytes, const int32_t* ids, int64_t count,
+                           void* sink, umapb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,8 @@ SIGNATURES = {
     "umapb_nnd_random_start_workspace": [_i64, _i32, _i32, _i32, _i32, _psz],
     "umapb_nnd_random_start": [_p, _i64, _i32, _i32, _p, _p, _i32, _p, _i32, _p, _sz, _p],
     "umapb_mt_jump_poly": [_i32, _p, _c.POINTER(_i64)],
+    "umapb_probe_random_access": [_p, _p, _i64, _i32, _i64, _i32, _i32, _p, _p],
+    "umapb_probe_row_gather": [_p, _i64, _i32, _p, _i64, _p, _p],
     "umapb_legacy_normal_workspace": [_i64, _psz],
     "umapb_legacy_normal": [_p, _i64, _f64, _f64, _p, _p, _sz, _p],
     "umapb_layout_count_active": [_p, _p, _i64, _i32, _i64, _i32, _p, _p, _sz, _p],

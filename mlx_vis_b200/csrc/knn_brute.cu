@@ -26,6 +26,7 @@
 // 3. rerank: one warp per row merges its slots, keeps the best L by
 //            (score, index), recomputes those L distances exactly in FP32
 //            (sum of (x_i - x_j)^2) and writes the k nearest by (distance, index).
+// Lists of more than 128 candidates (L = k + extra > 128) go to knn_exact.cu.
 #include <cuda_bf16.h>
 #include <math.h>
 #include <stdlib.h>
@@ -34,6 +35,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "knn_exact.cuh"
 #include "tc.cuh"
 
 namespace umapb {
@@ -86,6 +88,8 @@ struct Plan {
   __nv_bfloat16* xb;  // B operand rows [-2 x~, h1, h2, h3]
   float* cand_s;
   int32_t* cand_i;
+  bool exact;       // k + extra > 128: the long-list path (knn_exact.cu)
+  knnx::Plan xp;
 };
 
 __host__ __device__ inline int64_t first_cta(int64_t tile, int64_t tiles, int64_t grid) {
@@ -122,7 +126,13 @@ static int make_plan(int64_t n, int64_t d, int k, int extra, void* ws, Plan& p, 
   p.L = k + extra;
   if (p.L > n - 1) p.L = (int)(n - 1);
   if (p.L < k) p.L = k;
-  if (p.L > 128) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute: k + extra must be <= 128 (got %d)", k + extra);
+  p.exact = p.L > 128;
+  if (p.exact) {  // exact distances for every pair, no candidate lists
+    int s = knnx::plan(n, d, k, p.L, r0, m, ws, p.xp);
+    p.ws_bytes = p.xp.bytes;
+    p.status = p.xp.status;
+    return s;
+  }
   p.lcap = p.L <= 32 ? 32 : (p.L <= 64 ? 64 : 128);
   // features + three norm columns, padded to whole 64-element K blocks so every
   // 128-byte TMA box row starts on a 128-byte boundary
@@ -961,6 +971,10 @@ extern "C" int umapb_knn_brute_workspace(int64_t n, int64_t d, int32_t k, int32_
 // The three stages of one call; with `ev` (4 events) each stage boundary is recorded.
 static int enqueue_knn(const float* X, int64_t n, int64_t d, int32_t k, int32_t squared, int32_t* out_idx,
                        float* out_dist, const knn::Plan& p, cudaStream_t stream, cudaEvent_t* ev) {
+  if (p.exact) {
+    if (ev) return set_error(UMAPB_ERR_UNSUPPORTED, "knn_brute_timed: k + extra must be <= 128");
+    return knnx::run(X, p.xp, squared, out_idx, out_dist, stream);
+  }
   int s;
   const int P = knn::next_pow2(p.slots * p.L);
   const int PL = knn::next_pow2(p.L);
@@ -1118,6 +1132,13 @@ extern "C" int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int
   void* scratch = nullptr;
   if ((s = scratch_address(&scratch))) return s;
   knn::make_plan(n, d, k, extra, scratch, p);
+  if (p.exact) {
+    if ((s = knnx::run(X, p.xp, squared, out_idx, out_dist, stream))) return s;
+    if (device_status)
+      UMAPB_CUDA_TRY(cudaMemcpyAsync(device_status, p.status, sizeof(int32_t), cudaMemcpyDeviceToDevice, stream),
+                     "knn_brute_noalloc: status copy");
+    return UMAPB_OK;
+  }
 
   const int P = knn::next_pow2(p.slots * p.L);
   const int PL = knn::next_pow2(p.L);

@@ -57,8 +57,10 @@ def test_workspace_queries_and_argument_errors(lib):
     assert nbytes >= 20000 * 784 * 2 + 20000 * 31 * 8
     with pytest.raises(_lib.UmapB200Error, match="k <= n-1"):
         _lib.query("umapb_knn_brute_workspace", 10, 4, 10, 16)
-    with pytest.raises(_lib.UmapB200Error, match="<= 128"):
-        _lib.query("umapb_knn_brute_workspace", 1000, 4, 100, 40)
+    # lists above 128 take the exact-tile path: split operand + one (R, n) tile
+    assert _lib.query("umapb_knn_brute_workspace", 1000, 4, 100, 40) >= 1000 * 3 * 64 * 2 + 128 * 1000 * 4
+    with pytest.raises(_lib.UmapB200Error, match="k must be <= 4096"):
+        _lib.query("umapb_knn_brute_workspace", 10000, 4, 4097, 16)
     assert _lib.query("umapb_fuzzy_workspace", 1000, 15) > 1000 * 15 * 8
     assert _lib.query("umapb_spectral_workspace", 100, 7, 1000, 100) > 0  # n_components up to 32
     with pytest.raises(_lib.UmapB200Error, match="dim <= 32"):

@@ -103,8 +103,41 @@ def test_brute_argument_errors():
         _lib.knn_brute(X, 10)
     with pytest.raises(_lib.UmapB200Error, match="k <= n-1"):
         _lib.knn_brute(X, 0)
-    with pytest.raises(_lib.UmapB200Error, match="<= 128"):
-        _lib.knn_brute(torch.zeros((500, 4), device="cuda"), 120, extra=16)
+    with pytest.raises(_lib.UmapB200Error, match="k must be <= 4096"):
+        _lib.knn_brute(torch.zeros((5000, 4), device="cuda"), 4097)
+
+
+@pytest.mark.parametrize("n,d,k,extra", [(3000, 64, 113, 16), (2500, 784, 300, 0), (1200, 37, 1199, 16),
+                                         (41000, 16, 130, 16)])
+def test_brute_long_lists_are_exact(n, d, k, extra):
+    """k + extra > 128 (_knn.py has no limit on k): exact FP32-level distance tiles
+    and a per-row radix select.  Against float64 exact kNN: the k-th distance per row
+    within 1e-5 relative, every returned distance equal to the float64 distance of
+    the returned index (1e-5 relative), indices distinct and never the row itself;
+    41,000 rows take the select that re-reads the tile from memory."""
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(n + k)
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    X[: n // 10] = X[n // 10: 2 * (n // 10)]  # exact duplicates: zero distances and ties
+    Xd = torch.from_numpy(X).cuda()
+    idx, dist = _lib.knn_brute(Xd, k, extra=extra)
+    idx, dist = idx.cpu().numpy(), dist.cpu().numpy().astype(np.float64)
+    rows = np.arange(n) if n <= 3000 else rng.choice(n, 400, replace=False)
+    X64 = X.astype(np.float64)
+    sq = (X64 ** 2).sum(1)
+    for i in rows:
+        d2 = np.maximum(sq[i] + sq - 2.0 * X64 @ X64[i], 0.0)
+        d2[i] = np.inf
+        kth = np.sqrt(np.partition(d2, k - 1)[k - 1])
+        got = idx[i]
+        assert len(set(got.tolist())) == k and i not in got
+        assert np.all(np.diff(dist[i]) >= 0)
+        np.testing.assert_allclose(dist[i], np.sqrt(d2[got]), rtol=1e-5, atol=1e-5 * np.sqrt(sq[i] + 1.0))
+        assert abs(dist[i, -1] - kth) <= 1e-5 * (kth + np.sqrt(sq[i]) + 1e-6)
+    # squared output is the square of the Euclidean one
+    _, d2 = _lib.knn_brute(Xd, k, extra=extra, squared=True)
+    np.testing.assert_allclose(np.sqrt(d2.cpu().numpy().astype(np.float64)), dist, rtol=1e-6, atol=1e-6)
 
 
 def test_compute_knn_nndescent_branch(golden):
