@@ -261,7 +261,7 @@ def access_probes(torch, n, row_sizes):
             ts.append(a.elapsed_time(b) * 1e-3)
         return min(ts)
 
-    table = torch.rand((n, 2), device=dev)
+    table = torch.zeros((n, 2), device=dev)  # the values do not matter, the addresses do
     dtab = torch.zeros((n, 2), device=dev)
     sink = torch.zeros(16, device=dev)
     threads = torch.cuda.get_device_properties(dev).multi_processor_count * 2048
@@ -269,10 +269,10 @@ def access_probes(torch, n, row_sizes):
     t = best(lambda: _lib.call("umapb_probe_random_access", _lib.ptr(table), _lib.ptr(dtab), n, 2, threads, per, red,
                                _lib.ptr(sink), s))
     random_rate = threads * (per + (per + red - 1) // red) / t
-    ids = torch.randint(0, n, (31 * n,), dtype=torch.int32, device=dev)
+    ids = torch.from_numpy(np.random.default_rng(0).integers(0, n, 31 * n, dtype=np.int32)).to(dev)
     rates = {}
     for rb in sorted(set(row_sizes)):
-        tab = torch.randint(0, 255, (n * rb,), dtype=torch.uint8, device=dev)
+        tab = torch.zeros(n * rb, dtype=torch.uint8, device=dev)
         t = best(lambda: _lib.call("umapb_probe_row_gather", _lib.ptr(tab), n, rb, _lib.ptr(ids), ids.numel(),
                                    _lib.ptr(sink), s))
         rates[rb] = ids.numel() * rb / t

@@ -63,5 +63,43 @@ def upload_async(X, dev: torch.device | None = None):
     return Xd, done
 
 
+def upload_blocks_async(X, dev: torch.device | None = None, blocks: int = 8):
+    """Like upload_async, with the host rows copied in `blocks` row blocks: returns
+    (tensor, done event, [(row_end, event), ...]) so that work on the first rows may
+    start while the rest is still on its way (one block and no events when X is
+    already on the device)."""
+    dev = dev or device()
+    if isinstance(X, torch.Tensor) and X.is_cuda:
+        Xd = to_device_f32(X, dev)
+        return Xd, None, []
+    if isinstance(X, torch.Tensor):
+        host = X.detach()
+        if host.dtype != torch.float32:
+            host = host.float()
+        host = host.contiguous()
+    else:
+        host = torch.from_numpy(np.ascontiguousarray(np.asarray(X, dtype=np.float32)))
+    if host.ndim != 2:
+        raise ValueError(f"expected a 2-D array (n_samples, n_features), got shape {tuple(host.shape)}")
+    if not host.is_pinned() and host.numel() * 4 >= (1 << 20):
+        host = host.pin_memory()
+    n = host.shape[0]
+    main = torch.cuda.current_stream(dev)
+    Xd = torch.empty(host.shape, dtype=torch.float32, device=dev)
+    side = torch.cuda.Stream(device=dev)
+    side.wait_stream(main)  # Xd's allocation is ordered on the current stream
+    marks = []
+    step = max(1, -(-n // max(1, blocks)))
+    with torch.cuda.stream(side):
+        for r0 in range(0, n, step):
+            r1 = min(n, r0 + step)
+            Xd[r0:r1].copy_(host[r0:r1], non_blocking=True)
+            e = torch.cuda.Event()
+            e.record(side)
+            marks.append((r1, e))
+    Xd.record_stream(side)
+    return Xd, marks[-1][1], marks
+
+
 def to_host(t: torch.Tensor) -> np.ndarray:
     return t.detach().cpu().numpy()

@@ -351,14 +351,19 @@ def _kp(k: int) -> int:
     return max(64, (int(k) + 63) // 64 * 64)
 
 
-def split3(S: torch.Tensor, mu=None, transpose: bool = False, kp: int | None = None):
+def split3(S: torch.Tensor, mu=None, transpose: bool = False, kp: int | None = None, out=None):
     """Split-precision operand rows of S (rows x cols, float32): S rows (K = cols) or,
     with ``transpose``, S columns (K = rows), mu subtracted per stored column.
-    Returns (bf16 tensor (operand rows, 3 kp), kp)."""
+    Returns (bf16 tensor (operand rows, 3 kp), kp); ``out``: a contiguous tensor of
+    that shape to write into (a row block of a larger split, say)."""
     S = _require(S, torch.float32, 2, "S")
     rows, cols = S.shape
     kp = _kp(rows if transpose else cols) if kp is None else int(kp)
-    out = torch.empty(((cols if transpose else rows), 3 * kp), dtype=torch.bfloat16, device=S.device)
+    shape = ((cols if transpose else rows), 3 * kp)
+    if out is None:
+        out = torch.empty(shape, dtype=torch.bfloat16, device=S.device)
+    elif tuple(out.shape) != shape or out.dtype != torch.bfloat16 or not out.is_contiguous():
+        raise ValueError(f"split3: out must be a contiguous bfloat16 tensor of shape {shape}")
     if mu is not None:
         mu = _require(mu, torch.float32, 1, "mu")
     call("umapb_split3", ptr(S), rows, cols, S.stride(0), ptr(mu), int(bool(transpose)), kp, ptr(out),
@@ -370,7 +375,7 @@ SPLIT_SLICE_K = 1024  # K values per accumulator slice when ksplit is chosen aut
 
 
 def gemm_split3(A3: torch.Tensor, B3: torch.Tensor, kp: int, ksplit: int | None = None, scale: float = 1.0,
-                status: torch.Tensor | None = None) -> torch.Tensor:
+                status: torch.Tensor | None = None, out: torch.Tensor | None = None) -> torch.Tensor:
     """C = A B^T (M x N, float32) from split operands (FP32-level products on tcgen05).
 
     The tensor cores add the products of one accumulator in FP32; over a long K
@@ -382,6 +387,12 @@ def gemm_split3(A3: torch.Tensor, B3: torch.Tensor, kp: int, ksplit: int | None 
     if ksplit is None:
         ksplit = max(1, min(4096, -(-int(kp) // SPLIT_SLICE_K)))
     st = torch.zeros(1, dtype=torch.int32, device=dev) if status is None else status
+    if out is not None:  # one slice straight into out (M x N, contiguous float32)
+        if ksplit != 1 or scale != 1.0 or tuple(out.shape) != (M, N) or out.dtype != torch.float32 \
+                or not out.is_contiguous():
+            raise ValueError("gemm_split3: out needs ksplit 1, scale 1 and a contiguous float32 (M, N) tensor")
+        call("umapb_gemm_split3", ptr(A3), ptr(B3), M, N, int(kp), 1, ptr(out), N, ptr(st), stream_handle())
+        return out
     C = torch.empty((ksplit, M, N), dtype=torch.float32, device=dev)
     call("umapb_gemm_split3", ptr(A3), ptr(B3), M, N, int(kp), int(ksplit), ptr(C), N, ptr(st), stream_handle())
     if ksplit == 1 and scale == 1.0:

@@ -135,15 +135,22 @@ class NNDescent:
         return self.neighbor_graph
 
     # ------------------------------------------------------------------
-    def build_device(self, X: torch.Tensor, x_ready=None):
+    def build_device(self, X: torch.Tensor, x_ready=None, x_blocks=None):
         """Device version of build: (idx int32, Euclidean dist float32) CUDA tensors.
 
         ``x_ready``: an event that X's upload records (see _device.upload_async);
-        the random start, which does not read X, runs before the wait on it."""
+        the random start, which does not read X, runs before the wait on it.
+        ``x_blocks``: [(row_end, event), ...] of an upload in row blocks
+        (_device.upload_blocks_async): the per-row preparation of a block then
+        starts as soon as its rows have arrived."""
         if not isinstance(X, torch.Tensor) or not X.is_cuda:
             X = to_device_f32(X)
+            x_ready, x_blocks = None, None
+        if x_blocks:
             x_ready = None
-        if x_ready is None:
+            if X.dtype != torch.float32 or not X.is_contiguous():
+                raise ValueError("x_blocks needs a contiguous float32 X")
+        elif x_ready is None:
             X = X.contiguous().float()
         n, d = X.shape
         if n < 2:
@@ -161,21 +168,53 @@ class NNDescent:
             torch.cuda.current_stream(dev).wait_event(x_ready)
             X = X.contiguous().float()
         dist = torch.empty((n, k), dtype=torch.float32, device=dev)
-        sq = torch.empty(n, dtype=torch.float32, device=dev)
-        call("umapb_nnd_sqnorms", ptr(X), n, d, 0, ptr(sq), s)
-        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
 
-        X3 = None
+        # per-row preparation, one row block at a time: squared norms, the split of X
+        # into BF16 parts, X @ P (iteration 0) and X @ P2 (iteration 1) on the tensor
+        # cores with FP32-level error, and the FP16 rows of the FP16 iterations.  With
+        # an upload in row blocks, a block starts once its rows are on the device.
+        later = self.n_iters > 1
+        sq = torch.empty(n, dtype=torch.float32, device=dev)
+        X3 = P3 = P23 = kp = None
+        X_low, sq_low = X, sq
+        X300 = sq300 = X300h = None
         if P is not None:
-            # X @ P on the tensor cores with FP32-level error; X's split operand is
-            # kept for X @ P2 in iteration 1
-            X3 = _lib.split3(X)
-            X_low = _lib.matmul(X, P, A3=X3)
+            kp = _lib._kp(d)
+            X3 = torch.empty((n, 3 * kp), dtype=torch.bfloat16, device=dev)
+            P3, _ = _lib.split3(P, transpose=True, kp=kp)
+            X_low = torch.empty((n, P.shape[1]), dtype=torch.float32, device=dev)
             sq_low = torch.empty(n, dtype=torch.float32, device=dev)
-            call("umapb_nnd_sqnorms", ptr(X_low), n, X_low.shape[1], 0, ptr(sq_low), s)
-        else:
-            X_low, sq_low = X, sq
-        P2_d = P2
+            if P2 is not None and later:
+                P23, _ = _lib.split3(P2, transpose=True, kp=kp)
+                X300 = torch.empty((n, P2.shape[1]), dtype=torch.float32, device=dev)
+                sq300 = torch.empty(n, dtype=torch.float32, device=dev)
+                ld300 = (P2.shape[1] + 7) // 8 * 8
+                X300h = torch.empty((n, ld300), dtype=torch.float16, device=dev)
+        ldh = (d + 7) // 8 * 8  # FP16 rows padded to 16-byte chunks
+        Xh = torch.empty((n, ldh), dtype=torch.float16, device=dev) if later else None
+        r0 = 0
+        for r1, ready in (x_blocks or [(n, None)]):
+            if ready is not None:
+                torch.cuda.current_stream(dev).wait_event(ready)
+            m = r1 - r0
+            if m <= 0:
+                continue
+            Xb = X[r0:r1]
+            call("umapb_nnd_sqnorms", ptr(Xb), m, d, 0, ptr(sq[r0:r1]), s)
+            if P3 is not None:
+                A3, _ = _lib.split3(Xb, kp=kp, out=X3[r0:r1])
+                _lib.gemm_split3(A3, P3, kp, ksplit=1, out=X_low[r0:r1])
+                call("umapb_nnd_sqnorms", ptr(X_low[r0:r1]), m, X_low.shape[1], 0, ptr(sq_low[r0:r1]), s)
+                if X300 is not None:
+                    _lib.gemm_split3(A3, P23, kp, ksplit=1, out=X300[r0:r1])
+                    call("umapb_nnd_sqnorms", ptr(X300[r0:r1]), m, X300.shape[1], 0, ptr(sq300[r0:r1]), s)
+                    call("umapb_nnd_to_half", ptr(X300[r0:r1]), m, X300.shape[1], X300h.shape[1], ptr(X300h[r0:r1]),
+                         s)
+            if Xh is not None:
+                call("umapb_nnd_to_half", ptr(Xb), m, d, ldh, ptr(Xh[r0:r1]), s)
+            r0 = r1
+        X3 = P3 = P23 = None  # the split operands are not needed after the projections
+        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
 
         # locality order of the rows (sorted by one random-projection coordinate):
         # rows and sources that run side by side then share most of their
@@ -190,7 +229,6 @@ class NNDescent:
         # (changed, evals) counters of every iteration, zeroed once: an iteration
         # launches no fill and the host reads both with one copy
         counters = torch.zeros((max(self.n_iters, 1), 2), dtype=torch.int64, device=dev)
-        Xh = None
         # blocked nn-of-nn join (full path); UMAPB_NND_JOIN=0 computes every
         # candidate distance inside the row kernel instead
         join_on = os.environ.get("UMAPB_NND_JOIN", "1") != "0"
@@ -218,11 +256,8 @@ class NNDescent:
             else:
                 if it == 0:
                     Xd, sqd = X_low, sq_low
-                elif it == 1 and P2_d is not None:
-                    Xd = _lib.matmul(X, P2_d, A3=X3 if X3 is not None else _lib.split3(X))
-                    X3 = None  # the split operand is not needed after the last projection
-                    sqd = torch.empty(n, dtype=torch.float32, device=dev)
-                    call("umapb_nnd_sqnorms", ptr(Xd), n, Xd.shape[1], 0, ptr(sqd), s)
+                elif it == 1 and X300 is not None:
+                    Xd, sqd = X300, sq300
                 else:
                     Xd, sqd = X, sq
                 use_half = it in (1, 2, 3, 4)
@@ -231,11 +266,10 @@ class NNDescent:
                 ldx = dd
                 if use_half:
                     ldx = (dd + 7) // 8 * 8  # FP16 rows padded to 16-byte chunks
-                    if Xd is X:
-                        if Xh is None:
-                            Xh = torch.empty((n, ldx), dtype=torch.float16, device=dev)
-                            call("umapb_nnd_to_half", ptr(X), n, d, ldx, ptr(Xh), s)
+                    if Xd is X and Xh is not None:
                         src = Xh
+                    elif Xd is X300:
+                        src = X300h
                     else:
                         src = torch.empty((n, ldx), dtype=torch.float16, device=dev)
                         call("umapb_nnd_to_half", ptr(Xd), n, dd, ldx, ptr(src), s)

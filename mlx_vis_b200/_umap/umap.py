@@ -35,7 +35,7 @@ import torch
 
 from mlx_vis_b200 import _lib
 from mlx_vis_b200._curve import find_ab_params
-from mlx_vis_b200._device import device, to_host, upload_async
+from mlx_vis_b200._device import device, to_host, upload_blocks_async
 from mlx_vis_b200._normalize import normalize_input
 
 
@@ -105,9 +105,10 @@ class UMAP:
         if self.normalize:
             Xh = X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else np.asarray(X, dtype=np.float32)
             X = normalize_input(np.asarray(Xh, dtype=np.float32), self.normalize).astype(np.float32)
-        # a host X is copied on a side stream; the draws below and NNDescent's
-        # random start do not read X and run while the copy is in flight
-        Xd, x_ready = upload_async(X, dev)
+        # a host X is copied on a side stream in row blocks; the draws below and
+        # NNDescent's random start do not read X and run while the copy is in
+        # flight, and NNDescent prepares each row block once it has arrived
+        Xd, x_ready, x_blocks = upload_blocks_async(X, dev)
         n, dim = Xd.shape
         if n < 2:
             raise ValueError("UMAP needs at least 2 samples")
@@ -117,6 +118,7 @@ class UMAP:
 
         if self.pca_dim is not None and dim > self.pca_dim:
             x_ready = self._wait(x_ready, dev)
+            x_blocks = None
             Xd = self._pca(Xd)
             ev.mark("pca")
 
@@ -130,7 +132,8 @@ class UMAP:
             nn = NNDescent(k=k, verbose=self.verbose,
                            random_state=self.random_state if self.random_state is not None else 42)
             nn.profile_kernels = self.profile_kernels
-            knn_idx, knn_dist = nn.build_device(Xd, x_ready=x_ready)
+            knn_idx, knn_dist = nn.build_device(Xd, x_ready=x_ready, x_blocks=x_blocks)
+            x_ready = None
             self.nndescent_ = nn
         else:
             x_ready = self._wait(x_ready, dev)

@@ -93,6 +93,24 @@ def test_nndescent_waits_for_the_upload_after_its_random_start(gauss2000):
     assert torch.equal(idx_a, idx_b) and torch.equal(dist_a, dist_b)
 
 
+@pytest.mark.parametrize("d", [64, 350])
+def test_nndescent_prepares_row_blocks_as_they_arrive(d):
+    """An upload in row blocks (upload_blocks_async): norms, split, both projections
+    and FP16 rows are made block by block as the rows arrive; the graph equals the
+    one built from a device-resident X (350 features run both projections)."""
+    import torch
+
+    from mlx_vis_b200 import NNDescent
+    from mlx_vis_b200._device import upload_blocks_async
+
+    X = np.random.default_rng(d).normal(size=(3001, d)).astype(np.float32)
+    Xd, done, blocks = upload_blocks_async(torch.from_numpy(X).pin_memory(), blocks=5)
+    assert done is not None and len(blocks) == 5 and blocks[-1][0] == 3001
+    idx_a, dist_a = NNDescent(k=15, random_state=3).build_device(Xd, x_blocks=blocks)
+    idx_b, dist_b = NNDescent(k=15, random_state=3).build_device(torch.from_numpy(X).cuda())
+    assert torch.equal(idx_a, idx_b) and torch.equal(dist_a, dist_b)
+
+
 def test_wide_embedding_keeps_neighbourhoods(gauss2000):
     """n_components above 4 (warp-per-row spectral init, warp-per-edge epochs): the
     embedding of the 10-cluster mixture stays trustworthy like the 2-d one."""
