@@ -676,6 +676,13 @@ __global__ void __launch_bounds__(kWarps * 32) join_f32_kernel(JoinArgs a) {
   }
 }
 
+// query-row region of a warp: the staged query row (row_bytes), or before it the
+// prefetched nn-of-nn distances (pre floats), whichever is larger, 16-byte multiple
+__host__ __device__ inline size_t iter_row_region(int row_bytes, int pre) {
+  const size_t a = (size_t)row_bytes, b = (size_t)pre * 4;
+  return ((a > b ? a : b) + 15) / 16 * 16;
+}
+
 // dedup hash (4 hcap bytes), later candidate distances (4 tcap) + to-do list (2 tcap)
 __host__ __device__ inline size_t iter_scratch_bytes(int tcap, int hcap) {
   const size_t a = (size_t)hcap * 4, b = (size_t)tcap * 6;
@@ -712,9 +719,11 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   const int64_t slot = (int64_t)blockIdx.x * kWarps + warp;
   if (slot >= a.n) return;
   const int64_t row = a.order ? (int64_t)a.order[slot] : slot;
-  // per warp: query row | candidate ids | scratch (the dedup hash table, then the
-  // candidate distances and the to-do list) | sources
-  const size_t xs_bytes = ((size_t)a.ldx * sizeof(T) + 15) / 16 * 16;
+  // per warp: query row (first the prefetched nn-of-nn distances of the join) |
+  // candidate ids | scratch (the dedup hash table, then the candidate distances and
+  // the to-do list) | sources
+  const int nn_cols = a.mc_new * a.j_nn;
+  const size_t xs_bytes = iter_row_region(a.ldx * (int)sizeof(T), a.nnbuf ? nn_cols : 0);
   const size_t scratch = iter_scratch_bytes(a.tcap, a.hcap);
   const size_t per_warp = xs_bytes + (size_t)a.tcap * 4 + scratch + 32 * 4;
   uint8_t* base = smem_raw + warp * per_warp;
@@ -728,6 +737,17 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   if (row >= a.n) return;
   const int k = a.k;
   const int32_t* orow = a.idx_old + row * k;
+  // the row's nn-of-nn distances from the join, copied into shared memory while
+  // the candidate ids and the dedup run (4-byte cp.async: a row starts at any
+  // multiple of 4 bytes); phase 3 reads them from there
+  float* snn = reinterpret_cast<float*>(base);
+  if (a.nnbuf) {
+    const float* src = a.nnbuf + row * nn_cols;
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(snn));
+    for (int t = lane; t < nn_cols; t += 32)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + 4u * t), "l"(src + t) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
 
   // row-local copy of the old neighbours (lane p holds entry p; k <= 32)
   const int my_old = lane < k ? orow[lane] : -1;
@@ -756,7 +776,6 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   __syncwarp();
 
   // 1. candidate ids in the reference's column order
-  const int nn_cols = a.mc_new * a.j_nn;
   const int T_total = k + nn_cols + (a.rev ? k : 0);
   // four chunks at a time: their loads are issued together, one round trip
   for (int g0 = 0; g0 < a.tcap; g0 += 128) {
@@ -809,6 +828,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   __syncwarp();  // the hash table is dead; its space becomes cd / todo
 
   // 3. stored distances and the list of distances to compute
+  if (a.nnbuf) {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncwarp();
+  }
   int n_todo = 0;
   for (int t0 = 0, ch = 0; t0 < a.tcap; t0 += 32, ++ch) {
     const int t = t0 + lane;
@@ -820,7 +843,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
         else if (a.curd && t < a.mc_new) d = a.curd[row * k + t];
         else need = true;
       } else if (a.nnbuf && t < k + nn_cols) {
-        d = a.nnbuf[row * nn_cols + (t - k)];
+        d = snn[t - k];
       } else if (a.curd && t >= k + nn_cols) {
         // reverse candidate j: this row sits at some position p of j's list, and
         // for p < mc_new the join computed d(j, row) = d(row, j) as curd[j][p]
@@ -927,8 +950,8 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
 
 using namespace umapb;
 
-static size_t iter_smem_per_warp(int ldx, int elem, int tcap, int hcap) {
-  return ((size_t)ldx * elem + 15) / 16 * 16 + (size_t)tcap * 4 + nnd::iter_scratch_bytes(tcap, hcap) + 32 * 4;
+static size_t iter_smem_per_warp(int ldx, int elem, int tcap, int hcap, int pre) {
+  return nnd::iter_row_region(ldx * elem, pre) + (size_t)tcap * 4 + nnd::iter_scratch_bytes(tcap, hcap) + 32 * 4;
 }
 
 namespace umapb {
@@ -1222,7 +1245,8 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.flags_new = flags_new;
   a.changed = changed;
   a.evals = evals;
-  const size_t smem = (size_t)nnd::kWarps * iter_smem_per_warp(ldx, half ? 2 : 4, a.tcap, a.hcap);
+  const size_t smem = (size_t)nnd::kWarps *
+                      iter_smem_per_warp(ldx, half ? 2 : 4, a.tcap, a.hcap, a.nnbuf ? mc_new * j_nn : 0);
   UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_iteration: row dimension too large for shared memory");
   {
     static std::mutex mu;
