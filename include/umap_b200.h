@@ -190,6 +190,15 @@ int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, in
                    const int32_t* order, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf, float* curd,
                    int32_t* rev_out, unsigned long long* evals, void* workspace, size_t workspace_bytes,
                    umapb_stream_t stream);
+/* umapb_nnd_join_new: the blocked join of the converging path (nndescent.py:103-126):
+ * the sources of row i are the first mc of its neighbours in NEW-first stable order
+ * (none for a row without a NEW flag, whose list the iteration keeps); FP32 rows of
+ * dd floats (pitch dd, dd % 4 == 0); nnbuf[i][p*j_nn + j] = d(i, idx_old[s_p][j])
+ * for the p-th source s_p; pass nnbuf (and no curd) to the converging
+ * umapb_nnd_iteration.  Workspace: umapb_nnd_join_workspace(n, k, mc). */
+int umapb_nnd_join_new(const float* X, const float* sq, int32_t dd, const int32_t* idx_old, const uint8_t* flags_old,
+                       const int32_t* order, int64_t n, int32_t k, int32_t mc, int32_t j_nn, float* nnbuf,
+                       unsigned long long* evals, void* workspace, size_t workspace_bytes, umapb_stream_t stream);
 int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half, const int32_t* idx_old,
                         const float* dist_old, const uint8_t* flags_old, const int32_t* rev, const int32_t* order,
                         const float* nnbuf, const float* curd, int64_t n, int32_t k,

@@ -53,6 +53,7 @@ SIGNATURES = {
     "umapb_nnd_reverse": [_p, _i64, _i32, _p, _p, _sz, _p],
     "umapb_nnd_join_workspace": [_i64, _i32, _i32, _psz],
     "umapb_nnd_join": [_p, _p, _i32, _i32, _i32, _p, _p, _i64, _i32, _i32, _i32, _p, _p, _p, _p, _p, _sz, _p],
+    "umapb_nnd_join_new": [_p, _p, _i32, _p, _p, _p, _i64, _i32, _i32, _i32, _p, _p, _p, _sz, _p],
     "umapb_nnd_iteration": [_p, _p, _i32, _i32, _i32, _p, _p, _p, _p, _p, _p, _p, _i64, _i32, _i32, _i32, _i32, _i32, _p,
                             _p,
                             _p, _p, _p, _p],

@@ -247,12 +247,22 @@ class NNDescent:
                 # converging path: FP32, full dimension, stored distances
                 if use_rev:
                     call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
+                # the nn-of-nn distances of the NEW-first sources from the blocked join
+                join = join_on and k <= JOIN_MAX_K and mc_conv > 0 and j_nn > 0 and d % 4 == 0
+                if join and nnbuf is None:
+                    nnbuf = torch.empty(n * k * k, dtype=torch.float32, device=dev)
+                    curd = torch.empty((n, k), dtype=torch.float32, device=dev)
+                    join_ws = _lib.workspace(query("umapb_nnd_join_workspace", n, k, k), dev)
                 ev[0].record() if ev else None
+                if join:
+                    call("umapb_nnd_join_new", ptr(X), ptr(sq), d, ptr(idx), ptr(flags), ptr(order), n, k, mc_conv,
+                         j_nn, ptr(nnbuf), ptr(evals), ptr(join_ws), join_ws.numel(), s)
                 call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
-                     ptr(rev if use_rev else None), ptr(order), ptr(None), ptr(None), n, k, mc_conv, j_nn, 1, 0,
-                     ptr(idx2), ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
+                     ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None), ptr(None), n, k,
+                     mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
-                info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4)
+                info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4,
+                            join=join)
             else:
                 if it == 0:
                     Xd, sqd = X_low, sq_low

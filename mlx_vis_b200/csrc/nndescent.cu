@@ -412,23 +412,53 @@ __device__ __forceinline__ void dists_f32(const float* __restrict__ X, int dd, i
 // candidate: about mc + 1 + j_nn row reads per row instead of ~k + mc*j_nn + k.
 
 // entries: (i, p) with p < mc, bucketed by s = idx[i][p]; encoded i * 32 + p
-__global__ void src_count_kernel(const int32_t* __restrict__ idx, int64_t n, int k, int mc,
-                                 int32_t* __restrict__ cnt) {
-  const int64_t m = n * mc;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&cnt[idx[(t / mc) * k + (t % mc)]], 1);
+// The source of entry (i, p): idx[i][p], or srcs[i][p] when a source list is given
+// (negative: no source)
+__device__ __forceinline__ int entry_source(const int32_t* __restrict__ idx, const int32_t* __restrict__ srcs,
+                                            int64_t t, int k, int mc) {
+  return srcs ? srcs[t] : idx[(t / mc) * k + (t % mc)];
 }
 
-__global__ void src_fill_kernel(const int32_t* __restrict__ idx, int64_t n, int k, int mc,
-                                const int32_t* __restrict__ off, int32_t* __restrict__ fill,
+__global__ void src_count_kernel(const int32_t* __restrict__ idx, const int32_t* __restrict__ srcs, int64_t n, int k,
+                                 int mc, int32_t* __restrict__ cnt) {
+  const int64_t m = n * mc;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int sidx = entry_source(idx, srcs, t, k, mc);
+    if (sidx >= 0) atomicAdd(&cnt[sidx], 1);
+  }
+}
+
+__global__ void src_fill_kernel(const int32_t* __restrict__ idx, const int32_t* __restrict__ srcs, int64_t n, int k,
+                                int mc, const int32_t* __restrict__ off, int32_t* __restrict__ fill,
                                 int32_t* __restrict__ entries) {
   const int64_t m = n * mc;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x) {
+    const int sidx = entry_source(idx, srcs, t, k, mc);
+    if (sidx < 0) continue;
     const int64_t i = t / mc;
     const int p = (int)(t % mc);
-    const int sidx = idx[i * k + p];
     entries[off[sidx] + atomicAdd(&fill[sidx], 1)] = (int32_t)(i * 32 + p);
   }
+}
+
+// The converging path's sources (nndescent.py:103-107): the first mc of each row's
+// neighbours in NEW-first stable order, or none (-1) for a row without a NEW one
+// (its list stays as it is).  One warp per row, the row kernel's ordering rule.
+__global__ void new_sources_kernel(const int32_t* __restrict__ idx, const uint8_t* __restrict__ flags, int64_t n,
+                                   int k, int mc, int32_t* __restrict__ srcs) {
+  const int lane = threadIdx.x & 31;
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const bool f = lane < k && flags[row * k + lane];
+  const unsigned fb = __ballot_sync(0xffffffffu, f);
+  if (fb == 0) {
+    for (int p = lane; p < mc; p += 32) srcs[row * mc + p] = -1;
+    return;
+  }
+  const unsigned lt = (1u << lane) - 1u;
+  const unsigned ob = __ballot_sync(0xffffffffu, lane < k && !f);
+  const int pos = f ? __popc(fb & lt) : __popc(fb) + __popc(ob & lt);
+  if (lane < k && pos < mc) srcs[row * mc + pos] = idx[row * k + lane];
 }
 
 // work items: 16-entry chunks of each bucket (hub sources, listed by hundreds of
@@ -737,17 +767,6 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
   if (row >= a.n) return;
   const int k = a.k;
   const int32_t* orow = a.idx_old + row * k;
-  // the row's nn-of-nn distances from the join, copied into shared memory while
-  // the candidate ids and the dedup run (4-byte cp.async: a row starts at any
-  // multiple of 4 bytes); phase 3 reads them from there
-  float* snn = reinterpret_cast<float*>(base);
-  if (a.nnbuf) {
-    const float* src = a.nnbuf + row * nn_cols;
-    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(snn));
-    for (int t = lane; t < nn_cols; t += 32)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + 4u * t), "l"(src + t) : "memory");
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  }
 
   // row-local copy of the old neighbours (lane p holds entry p; k <= 32)
   const int my_old = lane < k ? orow[lane] : -1;
@@ -771,6 +790,17 @@ __global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
     if (lane < k) srcs[pos] = my_old;
   } else {
     if (lane < k) srcs[lane] = my_old;
+  }
+  // the row's nn-of-nn distances from the join, copied into shared memory while
+  // the candidate ids and the dedup run (4-byte cp.async: a row starts at any
+  // multiple of 4 bytes); phase 3 reads them from there
+  float* snn = reinterpret_cast<float*>(base);
+  if (a.nnbuf) {
+    const float* src = a.nnbuf + row * nn_cols;
+    const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(snn));
+    for (int t = lane; t < nn_cols; t += 32)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst + 4u * t), "l"(src + t) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
   for (int t = lane; t < a.hcap; t += 32) htab[t] = -1;
   __syncwarp();
@@ -1092,17 +1122,17 @@ extern "C" int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t
   c.take<int32_t>((size_t)n + 1);                // chunk counts -> chunk offsets
   c.take<int32_t>((size_t)n + (size_t)n * mc / 16 + 1);  // chunk -> source
   c.take<int64_t>(8);
+  c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));  // the NEW-first source lists (umapb_nnd_join_new)
   *bytes = c.bytes();
   return UMAPB_OK;
 }
 
-extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
-                              const int32_t* idx_old, const int32_t* order, int64_t n, int32_t k, int32_t mc,
-                              int32_t j_nn, float* nnbuf,
-                              float* curd, int32_t* rev_out, unsigned long long* evals, void* workspace,
-                              size_t workspace_bytes, umapb_stream_t stream_) {
-  clear_error();
-  cudaStream_t stream = reinterpret_cast<cudaStream_t>(stream_);
+// The blocked join over the sources idx_old[i][p < mc] or, with flags, over the
+// NEW-first source lists of the converging path (new_sources_kernel).
+static int join_impl(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
+                     const int32_t* idx_old, const uint8_t* flags, const int32_t* order, int64_t n, int32_t k,
+                     int32_t mc, int32_t j_nn, float* nnbuf, float* curd, int32_t* rev_out,
+                     unsigned long long* evals, void* workspace, size_t workspace_bytes, cudaStream_t stream) {
   UMAPB_REQUIRE(Xd && sqd && idx_old, "nnd_join: null array argument");
   UMAPB_REQUIRE(n >= 2 && dd >= 1 && ldx >= dd, "nnd_join: bad shape");
   UMAPB_REQUIRE(n < ((int64_t)1 << 26), "nnd_join: n must be below 2^26");
@@ -1125,6 +1155,7 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   const int64_t max_chunks = n + n * mc / 16;  // sum of ceil(count / 16) <= n + n*mc/16
   int32_t* chunk_pos = c.take<int32_t>((size_t)max_chunks + 1);
   int64_t* total = c.take<int64_t>(8);
+  int32_t* srcs = c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));
   if (!workspace || workspace_bytes < c.bytes())
     return set_error(UMAPB_ERR_WORKSPACE, "nnd_join: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
   if (mc == 0) return UMAPB_OK;
@@ -1133,9 +1164,13 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
   UMAPB_CUDA_TRY(cudaMemsetAsync(fill, 0, sizeof(int32_t) * (n + 1), stream), "nnd_join: reset");
   const int64_t want = ceil_div(m, 256);
   const unsigned blocks = (unsigned)(want < num_sms() * 8 ? want : num_sms() * 8);
-  nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off);
+  if (flags)
+    nnd::new_sources_kernel<<<(unsigned)ceil_div(n * 32, 256), 256, 0, stream>>>(idx_old, flags, n, k, mc, srcs);
+  else
+    srcs = nullptr;
+  nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, srcs, n, k, mc, off);
   scan_exclusive(off, n + 1, total, stream);
-  nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, n, k, mc, off, fill, entries);
+  nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, srcs, n, k, mc, off, fill, entries);
   if (rev_out) {  // with mc == k the buckets are the reverse-candidate buckets
     nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(
         entries, off, nullptr, n, k, 5, rev_out);
@@ -1169,18 +1204,42 @@ extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int3
     nnd::join_f16_kernel<<<jb, nnd::kWarps * 32, 0, stream>>>(a);
   } else {
     const size_t jsmem = (size_t)nnd::kWarps * nnd::JS_WARP_FLOATS * sizeof(float);
-    static bool js_attr = false;
-    if (!js_attr) {
+    static std::mutex mu;
+    static bool js_attr[64] = {false};
+    int dev = 0;
+    UMAPB_CUDA_TRY(cudaGetDevice(&dev), "nnd_join: device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || !js_attr[dev]) {
       UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::join_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)jsmem),
                      "nnd_join: smem attribute");
-      js_attr = true;
+      if (dev >= 0 && dev < 64) js_attr[dev] = true;
     }
     nnd::join_f32_kernel<<<jb, nnd::kWarps * 32, jsmem, stream>>>(a);
   }
   UMAPB_LAUNCH_CHECK("nnd_join kernels");
-  count_launches(rev_out ? 8 : 7);
+  count_launches((rev_out ? 8 : 7) + (flags ? 1 : 0));
   return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_join(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
+                              const int32_t* idx_old, const int32_t* order, int64_t n, int32_t k, int32_t mc,
+                              int32_t j_nn, float* nnbuf,
+                              float* curd, int32_t* rev_out, unsigned long long* evals, void* workspace,
+                              size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  return join_impl(Xd, sqd, dd, ldx, half, idx_old, nullptr, order, n, k, mc, j_nn, nnbuf, curd, rev_out, evals,
+                   workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream_));
+}
+
+extern "C" int umapb_nnd_join_new(const float* X, const float* sq, int32_t dd, const int32_t* idx_old,
+                                  const uint8_t* flags_old, const int32_t* order, int64_t n, int32_t k, int32_t mc,
+                                  int32_t j_nn, float* nnbuf, unsigned long long* evals, void* workspace,
+                                  size_t workspace_bytes, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(flags_old, "nnd_join_new: null flags");
+  return join_impl(X, sq, dd, dd, 0, idx_old, flags_old, order, n, k, mc, j_nn, nnbuf, nullptr, nullptr, evals,
+                   workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream_));
 }
 
 extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, int32_t half,
@@ -1222,7 +1281,7 @@ extern "C" int umapb_nnd_iteration(const void* Xd, const float* sqd, int32_t dd,
   a.flags_old = flags_old;
   a.rev = rev;
   a.order = order;
-  a.nnbuf = converging ? nullptr : nnbuf;
+  a.nnbuf = nnbuf;  // the converging path's comes from umapb_nnd_join_new
   a.curd = converging ? nullptr : curd;
   a.n = n;
   a.k = k;

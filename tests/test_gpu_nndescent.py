@@ -216,6 +216,46 @@ def test_join_block_distances(n, d, k, mc, j_nn, half):
         assert np.all(np.abs(got_nn.reshape(-1) - w2) <= tol2)
 
 
+@pytest.mark.parametrize("n,d,k,mc,j_nn", [(3000, 64, 15, 3, 7), (1000, 784, 15, 9, 15), (517, 36, 32, 20, 32),
+                                           (40, 8, 5, 3, 2)])
+def test_join_new_sources(n, d, k, mc, j_nn):
+    """umapb_nnd_join_new (converging path, nndescent.py:103-126): the sources of row i
+    are its first mc neighbours in NEW-first stable order, and nnbuf[i][p*j_nn + j] =
+    d(i, idx[s_p][j]) in FP32; rows without a NEW flag are left alone."""
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(n + d + k + mc)
+    X = rng.normal(size=(n, d)).astype(np.float32)
+    idx = rng.integers(0, n - 1, size=(n, k)).astype(np.int32)
+    idx = np.where(idx >= np.arange(n)[:, None], idx + 1, idx).astype(np.int32)
+    flags = (rng.random((n, k)) < 0.15).astype(np.uint8)
+    flags[: n // 4] = 0  # a quarter of the rows have no NEW neighbour
+    Xd = torch.from_numpy(X).cuda()
+    sq = torch.empty(n, dtype=torch.float32, device="cuda")
+    s = _lib.stream_handle()
+    _lib.call("umapb_nnd_sqnorms", _lib.ptr(Xd), n, d, 0, _lib.ptr(sq), s)
+    nnbuf = torch.full((n, mc * j_nn), -1.0, dtype=torch.float32, device="cuda")
+    evals = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ws = _lib.workspace(_lib.query("umapb_nnd_join_workspace", n, k, k), Xd.device)
+    order = torch.from_numpy(rng.permutation(n).astype(np.int32)).cuda() if n % 2 else None
+    d_idx, d_flags = torch.from_numpy(idx).cuda(), torch.from_numpy(flags).cuda()  # alive until the sync below
+    _lib.call("umapb_nnd_join_new", _lib.ptr(Xd), _lib.ptr(sq), d, _lib.ptr(d_idx), _lib.ptr(d_flags), _lib.ptr(order),
+              n, k, mc, j_nn, _lib.ptr(nnbuf), _lib.ptr(evals), _lib.ptr(ws), ws.numel(), s)
+    got = nnbuf.cpu().numpy()
+    X64 = X.astype(np.float64)
+    sqh = sq.cpu().numpy().astype(np.float64)
+    active = flags.any(1)
+    assert np.all(got[~active] == -1.0)
+    assert int(evals.item()) == int(active.sum()) * mc * (1 + j_nn)
+    for i in np.nonzero(active)[0][:300]:
+        newf = np.nonzero(flags[i])[0]
+        oldf = np.nonzero(flags[i] == 0)[0]
+        srcs = idx[i, np.concatenate([newf, oldf])][:mc]
+        cols = idx[np.repeat(srcs, j_nn), np.tile(np.arange(j_nn), mc)]
+        want = np.maximum(sqh[i] + sqh[cols] - 2.0 * (X64[cols] @ X64[i]), 0.0)
+        assert np.all(np.abs(got[i] - want) <= 1e-4 * (sqh[i] + sqh[cols]) + 1e-4)
+
+
 @pytest.mark.parametrize("name,gen", [("gauss", ("gaussian_mixture", 3000, 32, 2)),
                                       ("proto", ("prototype_mixture", 2000, 784, 3))])
 def test_join_and_row_kernel_builds_agree(name, gen, monkeypatch):
