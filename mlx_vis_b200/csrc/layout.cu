@@ -42,6 +42,11 @@ constexpr int kEdgesPerBlock = 1024;
 #endif
 // resident blocks per SM the epoch kernel is compiled for (register cap) and launched with
 constexpr int kEpochBlocksPerSM = UMAPB_LAYOUT_BLOCKS_PER_SM;
+#ifndef UMAPB_LAYOUT_BLOCKS_PER_SM5
+#define UMAPB_LAYOUT_BLOCKS_PER_SM5 4
+#endif
+// the same for the kernel specialised to 5 negatives per edge (the default rate)
+constexpr int kEpochBlocksPerSM5 = UMAPB_LAYOUT_BLOCKS_PER_SM5;
 constexpr int kPre = 8;  // epoch kernel: chunks of 32 edges whose schedule words load together
 
 // ---- reference pair math (float32, evaluation order of umap.py:361-383) ----
@@ -152,26 +157,29 @@ __global__ void eps_kernel(const float* __restrict__ vals, const int64_t* __rest
 // segment of edges, advances the schedule of the due ones and queues them in
 // shared memory; the warp works through the queue 32 edges at a time with every
 // lane busy (at most one partial batch per warp, at the end of its segment).
-template <int DIM>
-__device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* __restrict__ dY, int n,
-                                            const int32_t* __restrict__ rows, const int32_t* __restrict__ cols,
-                                            int64_t e, int epoch, const Params& p, int neg_rate, uint32_t k0,
+// NEG > 0: compiled for exactly NEG (<= 8) negatives per edge (neg_rate == NEG), so
+// the registers of the unused sample slots are not held.
+template <int DIM, int NEG>
+__device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* __restrict__ dY, int n, int i,
+                                            int j, int64_t e, int epoch, const Params& p, int neg_rate, uint32_t k0,
                                             uint32_t k1) {
-  const int i = rows[e], j = cols[e];
+  static_assert(NEG >= 0 && NEG <= 8, "NEG is 0 (any rate) or a rate <= 8");
   float yi[DIM], yj[DIM], acc[DIM], pos[DIM], neg_pos[DIM];
-  if (neg_rate <= 8) {
+  constexpr int kSlots = NEG > 0 ? NEG : 8;
+  const int nr = NEG > 0 ? NEG : neg_rate;
+  if (NEG > 0 || neg_rate <= 8) {
     // up to 8 negatives: draw their tails and issue every gather of Y before the
     // arithmetic, so the seven or so random reads of an edge are in flight together
     const U4 r0 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 0u}, k0, k1);
     U4 r1 = r0;
-    if (neg_rate > 4) r1 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 1u}, k0, k1);
+    if (nr > 4) r1 = philox4x32_10(U4{(uint32_t)e, (uint32_t)(e >> 32), (uint32_t)epoch, 1u}, k0, k1);
     const uint32_t rr[8] = {r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w};
-    float yt[8][DIM];
+    float yt[kSlots][DIM];
     load_row<DIM>(Y, i, yi);
     load_row<DIM>(Y, j, yj);
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (u < neg_rate) load_row<DIM>(Y, to_range(rr[u], (uint32_t)n), yt[u]);
+    for (int u = 0; u < kSlots; ++u)
+      if (u < nr) load_row<DIM>(Y, to_range(rr[u], (uint32_t)n), yt[u]);
     attract<DIM>(yi, yj, p, pos);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
@@ -179,8 +187,8 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
       neg_pos[c] = -pos[c];
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (u < neg_rate) repel_add<DIM>(yi, yt[u], p, acc);
+    for (int u = 0; u < kSlots; ++u)
+      if (u < nr) repel_add<DIM>(yi, yt[u], p, acc);
     atomic_add_row<DIM>(dY, j, neg_pos);
     atomic_add_row<DIM>(dY, i, acc);
     return;
@@ -210,8 +218,8 @@ __device__ __forceinline__ void edge_update(const float* __restrict__ Y, float* 
   atomic_add_row<DIM>(dY, i, acc);
 }
 
-template <int DIM>
-__global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY, int n,
+template <int DIM, int NEG>
+__global__ void __launch_bounds__(kBlock, NEG == 5 ? kEpochBlocksPerSM5 : kEpochBlocksPerSM) sgd_epoch_kernel(const float* __restrict__ Y, float* __restrict__ dY, int n,
                                                            const int32_t* __restrict__ rows,
                                                            const int32_t* __restrict__ cols,
                                                            const float* __restrict__ eps, float* __restrict__ next,
@@ -256,9 +264,31 @@ __global__ void __launch_bounds__(kBlock, kEpochBlocksPerSM) sgd_epoch_kernel(co
       if (due) bq[slot + __popc(b & below)] = (int32_t)(e - b0);
     }
     __syncthreads();
+    // the warp's batches: the head and tail ids of the next batch load while this
+    // batch's rows of Y are gathered, one round trip per batch instead of two
     const int total = s_cnt;
-    for (int base = warp * 32; base < total; base += kBlock)
-      if (base + lane < total) edge_update<DIM>(Y, dY, n, rows, cols, b0 + bq[base + lane], epoch, p, neg_rate, k0, k1);
+    int base = warp * 32;
+    int64_t e = 0;
+    int i = 0, j = 0;
+    if (base + lane < total) {
+      e = b0 + bq[base + lane];
+      i = rows[e];
+      j = cols[e];
+    }
+    for (; base < total; base += kBlock) {
+      const int nb = base + kBlock;
+      int64_t e2 = 0;
+      int i2 = 0, j2 = 0;
+      if (nb + lane < total) {
+        e2 = b0 + bq[nb + lane];
+        i2 = rows[e2];
+        j2 = cols[e2];
+      }
+      if (base + lane < total) edge_update<DIM, NEG>(Y, dY, n, i, j, e, epoch, p, neg_rate, k0, k1);
+      e = e2;
+      i = i2;
+      j = j2;
+    }
     __syncthreads();
   }
 }
@@ -528,9 +558,9 @@ static unsigned edge_grid(int64_t e_cap) {
 }
 
 // a few resident blocks per SM: long warp segments keep the partial batches rare
-static unsigned epoch_grid(int64_t e_cap) {
+static unsigned epoch_grid(int64_t e_cap, int blocks_per_sm) {
   const int64_t want = ceil_div(e_cap > 0 ? e_cap : 1, kBlock * 4);
-  const int64_t cap = (int64_t)num_sms() * kEpochBlocksPerSM;
+  const int64_t cap = (int64_t)num_sms() * blocks_per_sm;
   return (unsigned)(want < cap ? want : cap);
 }
 
@@ -538,9 +568,12 @@ template <int DIM>
 static void launch_epoch(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
                          const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
                          const Params& p, int neg_rate, uint64_t seed, cudaStream_t stream) {
-  sgd_epoch_kernel<DIM><<<epoch_grid(e_cap), kBlock, 0, stream>>>(Y, l.dY, (int)n, rows, cols, eps, next, n_edges,
-                                                                 epoch, p, neg_rate, (uint32_t)seed,
-                                                                 (uint32_t)(seed >> 32));
+  if (neg_rate == 5)
+    sgd_epoch_kernel<DIM, 5><<<epoch_grid(e_cap, kEpochBlocksPerSM5), kBlock, 0, stream>>>(
+        Y, l.dY, (int)n, rows, cols, eps, next, n_edges, epoch, p, neg_rate, (uint32_t)seed, (uint32_t)(seed >> 32));
+  else
+    sgd_epoch_kernel<DIM, 0><<<epoch_grid(e_cap, kEpochBlocksPerSM), kBlock, 0, stream>>>(
+        Y, l.dY, (int)n, rows, cols, eps, next, n_edges, epoch, p, neg_rate, (uint32_t)seed, (uint32_t)(seed >> 32));
   const int64_t m = n * DIM;
   const unsigned gb = (unsigned)(ceil_div(m, kBlock) < num_sms() * 8 ? ceil_div(m, kBlock) : num_sms() * 8);
   apply_kernel<<<gb, kBlock, 0, stream>>>(Y, l.dY, m);
