@@ -238,6 +238,10 @@ class NNDescent:
         t0 = time.time()
         update_frac = 1.0
         self.history_ = []
+        # FP32 distances of the current lists are due after the last FP16 iteration
+        # (nndescent.py:376-378): a following full FP32 iteration takes them from its
+        # join (every list position is a source there), anything else from a gather
+        fp32_due = False
         for it in range(self.n_iters):
             mc_nn, j_nn, mc_conv = iteration_params(update_frac, k, mc)
             use_rev = update_frac >= 0.10
@@ -245,6 +249,9 @@ class NNDescent:
             ev = self._events()
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
+                if fp32_due:
+                    call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 0, s)
+                    fp32_due = False
                 if use_rev:
                     call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
                 # the nn-of-nn distances of the NEW-first sources from the blocked join
@@ -273,6 +280,13 @@ class NNDescent:
                 use_half = it in (1, 2, 3, 4)
                 recompute = (it == 0) or use_half
                 dd = Xd.shape[1]
+                if fp32_due:
+                    if not (Xd is X and not use_half and join_on and k <= JOIN_MAX_K and mc_nn == k
+                            and d % 4 == 0):
+                        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 0, s)
+                    else:
+                        recompute = True  # the join's current-neighbour distances (curd)
+                    fp32_due = False
                 ldx = dd
                 if use_half:
                     ldx = (dd + 7) // 8 * 8  # FP16 rows padded to 16-byte chunks
@@ -306,7 +320,7 @@ class NNDescent:
                      ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
                 ev[1].record() if ev else None
                 if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)
-                    call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx2), ptr(dist2), k, 0, s)
+                    fp32_due = True
                 info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd,
                             elem=2 if use_half else 4, join=join)
             n_changed, n_evals = counters[it].tolist()  # the one host read per iteration
@@ -326,6 +340,8 @@ class NNDescent:
                 if self.verbose:
                     print(f"Converged at iteration {it + 1}")
                 break
+        if fp32_due:  # the loop stopped after the last FP16 iteration
+            call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 0, s)
         np.random.set_state(words_state(rng_state.cpu().numpy()))
         out = torch.empty_like(dist)
         _sqrt_into(dist, out)

@@ -564,11 +564,18 @@ static unsigned epoch_grid(int64_t e_cap, int blocks_per_sm) {
   return (unsigned)(want < cap ? want : cap);
 }
 
+// The kernel compiled for 5 negatives runs at that rate unless the environment sets
+// UMAPB_LAYOUT_NEG5=0 (read per call): both kernels make the same draws and sums.
+static bool neg5_kernel_enabled() {
+  const char* e = getenv("UMAPB_LAYOUT_NEG5");
+  return !(e && e[0] == '0' && e[1] == 0);
+}
+
 template <int DIM>
 static void launch_epoch(const Layout& l, float* Y, int64_t n, const int32_t* rows, const int32_t* cols,
                          const float* eps, float* next, const int64_t* n_edges, int64_t e_cap, int epoch,
-                         const Params& p, int neg_rate, uint64_t seed, cudaStream_t stream) {
-  if (neg_rate == 5)
+                         const Params& p, int neg_rate, uint64_t seed, bool neg5, cudaStream_t stream) {
+  if (neg_rate == 5 && neg5)
     sgd_epoch_kernel<DIM, 5><<<epoch_grid(e_cap, kEpochBlocksPerSM5), kBlock, 0, stream>>>(
         Y, l.dY, (int)n, rows, cols, eps, next, n_edges, epoch, p, neg_rate, (uint32_t)seed, (uint32_t)(seed >> 32));
   else
@@ -651,13 +658,14 @@ static int enqueue_epochs(float* Y, int64_t n, int32_t dim, const int32_t* rows,
     return set_error(UMAPB_ERR_WORKSPACE, "layout: workspace of %zu bytes, need %zu", workspace_bytes, l.bytes);
   l = layout::carve(workspace, n, dim, e_cap);
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epochs: reset");
+  const bool neg5 = layout::neg5_kernel_enabled();
   for (int ep = epoch_begin; ep < epoch_end; ++ep) {
     const layout::Params p = layout::make_params(a, b, learning_rate, ep, n_epochs);
     switch (dim) {
-      case 1: layout::launch_epoch<1>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
-      case 2: layout::launch_epoch<2>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
-      case 3: layout::launch_epoch<3>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
-      case 4: layout::launch_epoch<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream); break;
+      case 1: layout::launch_epoch<1>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, neg5, stream); break;
+      case 2: layout::launch_epoch<2>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, neg5, stream); break;
+      case 3: layout::launch_epoch<3>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, neg5, stream); break;
+      case 4: layout::launch_epoch<4>(l, Y, n, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, neg5, stream); break;
       default:
         layout::launch_epoch_wide(l, Y, n, dim, rows, cols, eps, next, n_edges, e_cap, ep, p, neg_rate, seed, stream);
         break;

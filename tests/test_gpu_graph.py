@@ -237,3 +237,26 @@ def test_graph_epochs_match_launched_epochs(golden, manifest):
     for o in outs[1:]:
         assert np.median(np.abs(o - outs[0])) < 1e-5 * scale
         assert np.abs(o - outs[0]).max() < 1e-2 * scale
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_neg5_kernel_matches_general_kernel(golden, manifest, monkeypatch, dim):
+    """At the default 5 negatives per edge the epochs run on a kernel compiled for that
+    rate (UMAPB_LAYOUT_NEG5=0 selects the general kernel): both draw the same tails and
+    make the same sums, so only the order of the float atomics may differ."""
+    fz, opt = golden("fuzzy_gauss"), golden("optimize_gauss")
+    m = manifest["optimize_gauss"]
+    Y0 = opt["Y_ep0"]
+    if dim != Y0.shape[1]:
+        Y0 = np.concatenate([Y0, Y0[:, :1] * 0.5], axis=1)[:, :dim].astype(np.float32)
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("UMAPB_LAYOUT_NEG5", flag)
+        lay = _layout(fz, dim=dim)
+        Y = cuda(Y0.copy())
+        lay.epochs(Y, 0, 6, m["a"], m["b"], 1.0, 5, 11, graph=False)
+        outs.append(Y.cpu().numpy())
+    scale = float(np.abs(outs[0]).max())
+    assert np.abs(outs[0] - Y0).max() > 1e-3 * scale
+    assert np.median(np.abs(outs[1] - outs[0])) < 1e-5 * scale
+    assert np.abs(outs[1] - outs[0]).max() < 1e-2 * scale
