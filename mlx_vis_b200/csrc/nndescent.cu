@@ -584,10 +584,7 @@ __global__ void __launch_bounds__(kWarps * 32) join_f16_kernel(JoinArgs a) {
 // float4 reads feed 64 FMAs), and one shuffle per output adds the halves.  A row
 // pitch of 40 floats puts the eight 16-byte reads of each instruction on distinct
 // bank groups.
-#ifndef UMAPB_JS_STAGES
-#define UMAPB_JS_STAGES 2
-#endif
-constexpr int JS_STAGES = UMAPB_JS_STAGES;
+constexpr int JS_STAGES = 2;
 constexpr int JS_SLICE = 32;  // floats of each row per stage
 constexpr int JS_PITCH = 40;  // floats per staged row
 constexpr int JS_WARP_FLOATS = JS_STAGES * 32 * JS_PITCH;
@@ -601,10 +598,9 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-#ifndef UMAPB_JS_MINB
-#define UMAPB_JS_MINB 1
-#endif
-__global__ void __launch_bounds__(kWarps * 32, UMAPB_JS_MINB) join_f32_kernel(JoinArgs a) {
+// 4 resident blocks per SM (at most 128 registers): with two stages the shared memory
+// of 4 blocks fits, and the issue-bound kernel wants the warps
+__global__ void __launch_bounds__(kWarps * 32, 4) join_f32_kernel(JoinArgs a) {
   extern __shared__ __align__(16) float js_smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
