@@ -519,7 +519,9 @@ __device__ __forceinline__ void join_store(const JoinArgs& a, int64_t s, int ent
 // entry rows g, g + 8 and of column rows g, g + 8, so A and B share the map and
 // D[m][n] is the full dot product.  D fragments: d0 = columns 2c, 2c + 1 of rows
 // g, g + 8; d1 = columns 8 + 2c, 9 + 2c.
-__global__ void __launch_bounds__(kWarps * 32) join_f16_kernel(JoinArgs a) {
+// 10 resident blocks per SM (48 registers, a few spilled to L1) rather than the 8 that
+// 60 registers allow: more row loads in flight for a kernel bound by them
+__global__ void __launch_bounds__(kWarps * 32, 10) join_f16_kernel(JoinArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t w = (int64_t)blockIdx.x * kWarps + warp;  // chunk
   if (w >= a.choff[a.n]) return;
