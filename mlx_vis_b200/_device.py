@@ -53,7 +53,7 @@ def upload_async(X, dev: torch.device | None = None):
         host = host.pin_memory()
     main = torch.cuda.current_stream(dev)
     Xd = torch.empty(host.shape, dtype=torch.float32, device=dev)
-    side = torch.cuda.Stream(device=dev)
+    side = copy_stream(dev)
     side.wait_stream(main)  # Xd's allocation is ordered on the current stream
     with torch.cuda.stream(side):
         Xd.copy_(host, non_blocking=True)
@@ -86,7 +86,7 @@ def upload_blocks_async(X, dev: torch.device | None = None, blocks: int = 8):
     n = host.shape[0]
     main = torch.cuda.current_stream(dev)
     Xd = torch.empty(host.shape, dtype=torch.float32, device=dev)
-    side = torch.cuda.Stream(device=dev)
+    side = copy_stream(dev)
     side.wait_stream(main)  # Xd's allocation is ordered on the current stream
     marks = []
     step = max(1, -(-n // max(1, blocks)))
@@ -99,6 +99,19 @@ def upload_blocks_async(X, dev: torch.device | None = None, blocks: int = 8):
             marks.append((r1, e))
     Xd.record_stream(side)
     return Xd, marks[-1][1], marks
+
+
+_copy_streams: dict = {}
+
+
+def copy_stream(dev: torch.device) -> torch.cuda.Stream:
+    """The side stream host uploads use on `dev`, made once per device (creating a
+    stream per fit costs host time between fits)."""
+    key = dev.index if dev.index is not None else torch.cuda.current_device()
+    st = _copy_streams.get(key)
+    if st is None:
+        st = _copy_streams[key] = torch.cuda.Stream(device=dev)
+    return st
 
 
 def to_host(t: torch.Tensor) -> np.ndarray:

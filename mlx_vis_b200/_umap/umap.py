@@ -92,12 +92,14 @@ class UMAP:
     # ------------------------------------------------------------------
     def fit_transform(self, X, epoch_callback=None) -> np.ndarray:
         """Fit UMAP and return the embedding (host float32, (n, n_components))."""
-        Y = self.fit_transform_device(X, epoch_callback=epoch_callback)
-        self.embedding_ = to_host(Y)
+        self._fit(X, epoch_callback, host_out=True)
         return self.embedding_
 
     def fit_transform_device(self, X, epoch_callback=None) -> torch.Tensor:
         """Like fit_transform but returns the CUDA tensor (no device-to-host copy)."""
+        return self._fit(X, epoch_callback, host_out=False)
+
+    def _fit(self, X, epoch_callback, host_out: bool) -> torch.Tensor:
         if self.n_components < 1 or self.n_components > 32:
             raise ValueError("n_components must be between 1 and 32")
         dev = device()
@@ -160,9 +162,24 @@ class UMAP:
 
         self._optimize(rows, cols, vals, n_edges, Y, a, b, n, seed, epoch_callback)
         ev.mark("layout")
-        self.timings_ = ev.finish()
-        self.graph_info_ = {"n_edges": int(n_edges.item())}
-        if self._spectral_ws is not None and _lib.status_word(self._spectral_ws) != 0:
+        # the values the host reads after the fit (edge count, spectral status, the
+        # embedding for fit_transform) are copied into pinned memory on the stream,
+        # so one synchronisation serves them all
+        ne_h = torch.empty(1, dtype=torch.int64, pin_memory=True)
+        ne_h.copy_(n_edges.reshape(-1)[:1], non_blocking=True)
+        st_h = None
+        if self._spectral_ws is not None:
+            st_h = torch.empty(1, dtype=torch.int32, pin_memory=True)
+            st_h.copy_(self._spectral_ws[:4].view(torch.int32), non_blocking=True)
+        Y_h = None
+        if host_out:
+            Y_h = torch.empty(Y.shape, dtype=Y.dtype, pin_memory=True)
+            Y_h.copy_(Y, non_blocking=True)
+        self.timings_ = ev.finish()  # synchronises the device
+        self.graph_info_ = {"n_edges": int(ne_h[0])}
+        if Y_h is not None:
+            self.embedding_ = Y_h.numpy()
+        if st_h is not None and int(st_h[0]) != 0:
             # the power iteration's bounded grid barrier gave up; the device already
             # replaced Y by the random start (umap.py:354-357)
             self.init_used_ = "random"

@@ -175,6 +175,7 @@ struct Layout {
   float* w_sym;
   float* wmax;
   int32_t* block_counts;
+  int64_t* scan_ws;  // scan_exclusive's block totals
   size_t bytes;
 };
 
@@ -186,6 +187,7 @@ static Layout carve(void* ws, int64_t n, int k) {
   l.w_sym = c.take<float>((size_t)n * k);
   l.wmax = c.take<float>(64);
   l.block_counts = c.take<int32_t>((size_t)ceil_div(n * k, kEdgesPerBlock) + 1);
+  l.scan_ws = c.take<int64_t>(kScanMaxBlocks);
   l.bytes = c.bytes();
   return l;
 }
@@ -232,7 +234,7 @@ extern "C" int umapb_fuzzy(const int32_t* knn_idx, const float* knn_dist, int64_
   const int64_t nb = ceil_div(m, fuzzy::kEdgesPerBlock);
   fuzzy::prune_count_kernel<<<(unsigned)nb, fuzzy::kBlock, 0, stream>>>(l.w_sym, m, l.wmax, n_epochs, l.block_counts);
   UMAPB_LAUNCH_CHECK("fuzzy: prune count kernel");
-  scan_exclusive(l.block_counts, nb, n_edges, stream);
+  scan_exclusive(l.block_counts, nb, n_edges, l.scan_ws, stream);
   UMAPB_LAUNCH_CHECK("fuzzy: scan kernel");
   fuzzy::prune_write_kernel<<<(unsigned)nb, fuzzy::kBlock, 0, stream>>>(l.w_sym, knn_idx, m, k, l.wmax, n_epochs,
                                                                        l.block_counts, rows, cols, vals);

@@ -525,6 +525,7 @@ struct Layout {
   float* wmax;
   int32_t* block_counts;
   int64_t* total;
+  int64_t* scan_ws;  // scan_exclusive's block totals
   size_t bytes;
 };
 
@@ -536,6 +537,7 @@ static Layout carve(void* ws, int64_t n, int dim, int64_t e_cap) {
   l.dY = c.take<float>((size_t)n * dim);
   l.block_counts = c.take<int32_t>((size_t)ceil_div(e_cap > 0 ? e_cap : 1, kEdgesPerBlock) + 1);
   l.total = c.take<int64_t>(8);
+  l.scan_ws = c.take<int64_t>(kScanMaxBlocks);
   l.bytes = c.bytes();
   return l;
 }
@@ -759,7 +761,7 @@ extern "C" int umapb_layout_count_active(const float* next, const int64_t* n_edg
   l = layout::carve(workspace, n, dim, e_cap);
   const int64_t nb = ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
   layout::count_active_kernel<<<(unsigned)nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
-  scan_exclusive(l.block_counts, nb, count, stream);
+  scan_exclusive(l.block_counts, nb, count, l.scan_ws, stream);
   UMAPB_LAUNCH_CHECK("layout_count_active kernels");
   count_launches(2);
   return UMAPB_OK;
@@ -785,7 +787,7 @@ extern "C" int umapb_layout_epoch_injected(float* Y, int64_t n, int32_t dim, con
   UMAPB_CUDA_TRY(cudaMemsetAsync(l.dY, 0, sizeof(float) * n * dim, stream), "layout_epoch_injected: reset");
   const unsigned nb = (unsigned)ceil_div(e_cap > 0 ? e_cap : 1, layout::kEdgesPerBlock);
   layout::count_active_kernel<<<nb, layout::kBlock, 0, stream>>>(next, n_edges, epoch, l.block_counts);
-  scan_exclusive(l.block_counts, (int64_t)nb, l.total, stream);
+  scan_exclusive(l.block_counts, (int64_t)nb, l.total, l.scan_ws, stream);
   UMAPB_LAUNCH_CHECK("layout_epoch_injected: active count");
   int64_t active = 0;
   UMAPB_CUDA_TRY(cudaMemcpyAsync(&active, l.total, sizeof(active), cudaMemcpyDeviceToHost, stream),

@@ -184,6 +184,7 @@ struct SortLayout {
   int32_t* i[2];
   int32_t* counts;
   int64_t* total;
+  int64_t* scan_ws;  // scan_exclusive's block totals
   size_t bytes;
 };
 
@@ -197,6 +198,7 @@ static SortLayout sort_carve(void* ws, int64_t n) {
   }
   l.counts = c.take<int32_t>((size_t)(256 * tiles));
   l.total = c.take<int64_t>(1);
+  l.scan_ws = c.take<int64_t>(kScanMaxBlocks);
   l.bytes = c.bytes();
   return l;
 }
@@ -285,7 +287,7 @@ extern "C" int umapb_sort_keys(const float* keys, int64_t n, int64_t stride, int
   for (int pass = 0; pass < 4; ++pass) {
     const int src = pass & 1, dst = src ^ 1;
     linalg::sort_hist_kernel<<<(unsigned)tiles, linalg::kSortTile, 0, stream>>>(l.k[src], n, 8 * pass, l.counts);
-    scan_exclusive(l.counts, 256 * tiles, l.total, stream);
+    scan_exclusive(l.counts, 256 * tiles, l.total, l.scan_ws, stream);
     int32_t* iout = pass == 3 ? order : l.i[dst];
     linalg::sort_scatter_kernel<<<(unsigned)tiles, linalg::kSortTile, 0, stream>>>(
         l.k[src], l.i[src], n, 8 * pass, l.counts, l.k[dst], iout);

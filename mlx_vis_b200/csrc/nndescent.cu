@@ -1078,7 +1078,7 @@ extern "C" int umapb_nnd_reverse_workspace(int64_t n, int32_t k, size_t* bytes) 
   c.take<int32_t>((size_t)n + 1);  // fill counters
   c.take<int32_t>((size_t)n);      // degree copy
   c.take<int32_t>((size_t)n * k);  // buckets
-  c.take<int64_t>(8);
+  c.take<int64_t>(8 + kScanMaxBlocks);  // totals, then scan_exclusive's block totals
   *bytes = c.bytes();
   return UMAPB_OK;
 }
@@ -1095,7 +1095,7 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   int32_t* fill = c.take<int32_t>((size_t)n + 1);
   int32_t* deg = c.take<int32_t>((size_t)n);
   int32_t* bucket = c.take<int32_t>((size_t)n * k);
-  int64_t* total = c.take<int64_t>(8);
+  int64_t* total = c.take<int64_t>(8 + kScanMaxBlocks);  // total, then scan scratch at total + 8
   if (!workspace || workspace_bytes < c.bytes())
     return set_error(UMAPB_ERR_WORKSPACE, "nnd_reverse: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
   const int64_t m = n * k;
@@ -1106,7 +1106,7 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
   nnd::indegree_kernel<<<blocks, 256, 0, stream>>>(idx, m, off);
   UMAPB_CUDA_TRY(cudaMemcpyAsync(deg, off, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, stream),
                  "nnd_reverse: degree copy");
-  scan_exclusive(off, n, total, stream);
+  scan_exclusive(off, n, total, total + 8, stream);
   nnd::bucket_fill_kernel<<<blocks, 256, 0, stream>>>(idx, m, k, off, fill, bucket);
   nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
                                                                                                   n, k, 0, rev);
@@ -1125,7 +1125,7 @@ extern "C" int umapb_nnd_join_workspace(int64_t n, int32_t k, int32_t mc, size_t
   c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));  // entries
   c.take<int32_t>((size_t)n + 1);                // chunk counts -> chunk offsets
   c.take<int32_t>((size_t)n + (size_t)n * mc / 16 + 1);  // chunk -> source
-  c.take<int64_t>(8);
+  c.take<int64_t>(8 + kScanMaxBlocks);  // totals, then scan_exclusive's block totals
   c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));  // the NEW-first source lists (umapb_nnd_join_new)
   *bytes = c.bytes();
   return UMAPB_OK;
@@ -1158,7 +1158,7 @@ static int join_impl(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, 
   int32_t* choff = c.take<int32_t>((size_t)n + 1);
   const int64_t max_chunks = n + n * mc / 16;  // sum of ceil(count / 16) <= n + n*mc/16
   int32_t* chunk_pos = c.take<int32_t>((size_t)max_chunks + 1);
-  int64_t* total = c.take<int64_t>(8);
+  int64_t* total = c.take<int64_t>(8 + kScanMaxBlocks);  // total, then scan scratch at total + 8
   int32_t* srcs = c.take<int32_t>((size_t)n * (mc > 0 ? mc : 1));
   if (!workspace || workspace_bytes < c.bytes())
     return set_error(UMAPB_ERR_WORKSPACE, "nnd_join: workspace of %zu bytes, need %zu", workspace_bytes, c.bytes());
@@ -1173,7 +1173,7 @@ static int join_impl(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, 
   else
     srcs = nullptr;
   nnd::src_count_kernel<<<blocks, 256, 0, stream>>>(idx_old, srcs, n, k, mc, off);
-  scan_exclusive(off, n + 1, total, stream);
+  scan_exclusive(off, n + 1, total, total + 8, stream);
   nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, srcs, n, k, mc, off, fill, entries);
   if (rev_out) {  // with mc == k the buckets are the reverse-candidate buckets
     nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(
@@ -1182,7 +1182,7 @@ static int join_impl(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, 
   const unsigned sblocks = (unsigned)ceil_div(n, 256);
   UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
   nnd::chunk_count_kernel<<<sblocks, 256, 0, stream>>>(off, order, n, choff);
-  scan_exclusive(choff, n + 1, total, stream);
+  scan_exclusive(choff, n + 1, total, total + 8, stream);
   nnd::chunk_fill_kernel<<<sblocks, 256, 0, stream>>>(choff, n, chunk_pos);
   nnd::JoinArgs a;
   a.Xd = Xd;

@@ -772,6 +772,7 @@ struct Plan {
   uint32_t* part;    // (nseg - 1, kJumpParts, 624) partial start words of the segments
   int32_t* cnt_i;
   int32_t* cnt_a;
+  int64_t* scan_ws;  // scan_exclusive's block totals
 };
 
 // Words for `count` integers accepted with probability p = (rng + 1) / (mask + 1)
@@ -798,6 +799,7 @@ static Plan plan(void* ws, int64_t count, uint32_t rng, uint32_t mask, int64_t G
   p.part = c.take<uint32_t>((size_t)(p.nseg - 1) * kJumpParts * kN);
   p.cnt_i = c.take<int32_t>((size_t)p.nbI + 1);
   p.cnt_a = c.take<int32_t>((size_t)p.nbA + 1);
+  p.scan_ws = c.take<int64_t>(kScanMaxBlocks);
   p.bytes = c.bytes();
   return p;
 }
@@ -823,14 +825,14 @@ static int run_parallel(const Plan& p, uint32_t* state, int64_t count, int k, ui
     ++launches;
   } else if (count > 0) {
     int_count_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i);
-    scan_exclusive(p.cnt_i, p.nbI, &p.sc->tot_int, stream);
+    scan_exclusive(p.cnt_i, p.nbI, &p.sc->tot_int, p.scan_ws, stream);
     int_scatter_kernel<<<(unsigned)p.nbI, kPar, 0, stream>>>(p.raw, state, p.Wi, rng, mask, p.cnt_i, count, k, idx,
                                                              p.sc);
     launches += 3;
   }
   if (G > 0) {
     att_count_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a);
-    scan_exclusive(p.cnt_a, p.nbA, &p.sc->tot_att, stream);
+    scan_exclusive(p.cnt_a, p.nbA, &p.sc->tot_att, p.scan_ws, stream);
     att_scatter_kernel<<<(unsigned)p.nbA, kPar, 0, stream>>>(p.raw, state, p.sc, p.Aw, p.cnt_a, G, out);
     launches += 3;
   }

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace umapb {
 
 constexpr int kScanThreads = 1024;
@@ -25,42 +27,59 @@ inline void scan_shape(int64_t count, int* blocks, int64_t* span) {
   *span = s;
 }
 
-// Exclusive scan of `count` int32 values in place, in ONE launch without any wait
-// between blocks: block b owns [b span, (b + 1) span) and first sums every value
-// before its range itself (16-byte loads, all in flight at once; at most
-// kScanMaxBlocks / 2 times the array is read again, from L2 at the sizes the
-// pipeline scans), then scans its range in passes of 16 K values: a thread scans its
-// 16 consecutive values in registers, the block scans the thread sums (warp
-// shuffles, then one warp over the 32 warp sums) and a running carry links the
-// passes.  The last block writes the grand total to *total.
+// Exclusive scan of `count` int32 values in place.  Block b owns [b span, (b + 1)
+// span).  With more than one block, a first launch writes each block's range total
+// to block_sums (it writes nothing to vals), and the scan launch starts block b from
+// the sum of block_sums[0, b); the launch boundary orders the two, so no block reads a
+// range another block is rewriting.  A block scans its range in passes of 16 K
+// values: a thread scans its 16 consecutive values in registers, the block scans the
+// thread sums (warp shuffles, then one warp over the 32 warp sums) and a running
+// carry links the passes.  The last block writes the grand total to *total.
+template <int kDummy = 0>
+__global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(const int32_t* __restrict__ vals,
+                                                                       int64_t count, int64_t span,
+                                                                       int64_t* __restrict__ block_sums) {
+  __shared__ int64_t warp_sums[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t lo = (int64_t)blockIdx.x * span;
+  const int64_t hi = lo + span < count ? lo + span : count;
+  int64_t s = 0;
+  if ((reinterpret_cast<uintptr_t>(vals) & 15) == 0) {
+    const int64_t hi4 = lo + (hi - lo) / 4 * 4;  // lo is a multiple of 16
+    for (int64_t i = lo + 4 * (int64_t)threadIdx.x; i < hi4; i += 4 * (int64_t)kScanThreads) {
+      const int4 a = *reinterpret_cast<const int4*>(vals + i);
+      s += (int64_t)a.x + a.y + a.z + a.w;
+    }
+    for (int64_t i = hi4 + threadIdx.x; i < hi; i += kScanThreads) s += vals[i];
+  } else {
+    for (int64_t i = lo + threadIdx.x; i < hi; i += kScanThreads) s += vals[i];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) warp_sums[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t t = 0;
+    for (int w = 0; w < kScanThreads / 32; ++w) t += warp_sums[w];
+    block_sums[blockIdx.x] = t;
+  }
+}
+
 template <int kDummy = 0>
 __global__ void __launch_bounds__(kScanThreads) scan_exclusive_kernel(int32_t* __restrict__ vals, int64_t count,
-                                                                      int64_t span, int64_t* __restrict__ total) {
+                                                                      int64_t span,
+                                                                      const int64_t* __restrict__ block_sums,
+                                                                      int64_t* __restrict__ total) {
   __shared__ int64_t warp_sums[32];
   __shared__ int64_t carry;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool aligned = (reinterpret_cast<uintptr_t>(vals) & 15) == 0;
   const int64_t lo = (int64_t)blockIdx.x * span;
   const int64_t hi = lo + span < count ? lo + span : count;
-
-  // the sum of vals[0, lo)
-  int64_t pre = 0;
-  if (aligned) {
-    for (int64_t i = 4 * (int64_t)threadIdx.x; i < lo; i += 4 * (int64_t)kScanThreads) {
-      const int4 a = *reinterpret_cast<const int4*>(vals + i);  // lo is a multiple of 16
-      pre += (int64_t)a.x + a.y + a.z + a.w;
-    }
-  } else {
-    for (int64_t i = threadIdx.x; i < lo; i += kScanThreads) pre += vals[i];
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
-  if (lane == 0) warp_sums[warp] = pre;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int64_t s = 0;
-    for (int w = 0; w < kScanThreads / 32; ++w) s += warp_sums[w];
-    carry = s;
+  if (threadIdx.x == 0) {  // the sum of vals[0, lo): the totals of the blocks before
+    int64_t c = 0;
+    for (int b = 0; b < (int)blockIdx.x; ++b) c += block_sums[b];
+    carry = c;
   }
   __syncthreads();
 
@@ -122,12 +141,17 @@ __global__ void __launch_bounds__(kScanThreads) scan_exclusive_kernel(int32_t* _
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *total = carry;
 }
 
-// Enqueue the scan of vals[0, count) (count >= 0) on `stream`.
-inline void scan_exclusive(int32_t* vals, int64_t count, int64_t* total, cudaStream_t stream) {
+// Enqueue the scan of vals[0, count) (count >= 0) on `stream`; block_sums is caller
+// scratch of kScanMaxBlocks int64 values (not read when one block covers count).
+inline void scan_exclusive(int32_t* vals, int64_t count, int64_t* total, int64_t* block_sums, cudaStream_t stream) {
   int blocks;
   int64_t span;
   scan_shape(count, &blocks, &span);
-  scan_exclusive_kernel<<<blocks, kScanThreads, 0, stream>>>(vals, count, span, total);
+  if (blocks > 1) {
+    scan_block_sums_kernel<<<blocks, kScanThreads, 0, stream>>>(vals, count, span, block_sums);
+    count_launches(1);  // the callers count the scan launch itself
+  }
+  scan_exclusive_kernel<<<blocks, kScanThreads, 0, stream>>>(vals, count, span, block_sums, total);
 }
 
 }  // namespace umapb
