@@ -119,6 +119,15 @@ int umapb_knn_brute_noalloc(const float* X, int64_t n, int64_t d, int32_t k, int
  *                     in FP32 (_gather_dists, nndescent.py:573-612); with
  *                     sort_rows != 0 each row is then sorted by (distance, id)
  *                     (the initial sort, nndescent.py:63-65).
+ * umapb_nnd_gather_pairs: the same distances for the pairs (i, j = idx[i][p]) with
+ *                     i < r1 whose later row max(i, j) lies in [r0, r1); called once
+ *                     per row block [r0, r1) of an upload in row order, it computes
+ *                     every pair once, as soon as both rows are on the device, with
+ *                     the same values umapb_nnd_gather gives.  idx is not changed.
+ *                     k <= 32.
+ * umapb_nnd_sort_rows: each row of (dist, idx) sorted by (distance, id), k <= 32; after
+ *                     the last block, the pair gathers and this equal
+ *                     umapb_nnd_gather with sort_rows != 0.
  * umapb_nnd_reverse:  reverse candidates (_compute_reverse_candidates,
  *                     nndescent.py:406-436): slot p of row j = p-th smallest source
  *                     i with j in idx[i], 0 when j has fewer in-edges.
@@ -182,6 +191,9 @@ int umapb_nnd_sqnorms(const void* X, int64_t n, int32_t dd, int32_t half, float*
 int umapb_nnd_to_half(const float* X, int64_t n, int32_t dd, int32_t ldh, void* H, umapb_stream_t stream);
 int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int32_t dd, int32_t* idx, float* dist, int32_t k,
                      int32_t sort_rows, umapb_stream_t stream);
+int umapb_nnd_gather_pairs(const float* X, const float* sq, int64_t n, int32_t dd, const int32_t* idx, float* dist,
+                           int32_t k, int64_t r0, int64_t r1, umapb_stream_t stream);
+int umapb_nnd_sort_rows(int32_t* idx, float* dist, int64_t n, int32_t k, umapb_stream_t stream);
 int umapb_nnd_reverse_workspace(int64_t n, int32_t k, size_t* bytes);
 int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32_t* rev, void* workspace,
                       size_t workspace_bytes, umapb_stream_t stream);

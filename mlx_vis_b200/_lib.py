@@ -49,6 +49,8 @@ SIGNATURES = {
     "umapb_nnd_sqnorms": [_p, _i64, _i32, _i32, _p, _p],
     "umapb_nnd_to_half": [_p, _i64, _i32, _i32, _p, _p],
     "umapb_nnd_gather": [_p, _p, _i64, _i32, _p, _p, _i32, _i32, _p],
+    "umapb_nnd_gather_pairs": [_p, _p, _i64, _i32, _p, _p, _i32, _i64, _i64, _p],
+    "umapb_nnd_sort_rows": [_p, _p, _i64, _i32, _p],
     "umapb_nnd_reverse_workspace": [_i64, _i32, _psz],
     "umapb_nnd_reverse": [_p, _i64, _i32, _p, _p, _sz, _p],
     "umapb_nnd_join_workspace": [_i64, _i32, _i32, _psz],

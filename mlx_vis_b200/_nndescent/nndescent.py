@@ -212,9 +212,15 @@ class NNDescent:
                          s)
             if Xh is not None:
                 call("umapb_nnd_to_half", ptr(Xb), m, d, ldh, ptr(Xh[r0:r1]), s)
+            if k <= JOIN_MAX_K:  # the random start's pairs whose later row is in this block
+                call("umapb_nnd_gather_pairs", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, r0, r1, s)
             r0 = r1
         X3 = P3 = P23 = None  # the split operands are not needed after the projections
-        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
+        # the random start's FP32 distances, each row sorted (nndescent.py:59-65)
+        if k <= JOIN_MAX_K:
+            call("umapb_nnd_sort_rows", ptr(idx), ptr(dist), n, k, s)
+        else:
+            call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 1, s)
 
         # locality order of the rows (sorted by one random-projection coordinate):
         # rows and sources that run side by side then share most of their

@@ -206,6 +206,60 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, const float* __r
   }
 }
 
+// The pairs (i, j = idx[i][p]) of rows i < r1 whose later row max(i, j) lies in
+// [r0, r1): launched once per row block of an upload in row order, every pair is
+// computed once, as soon as both of its rows are on the device, with the same
+// expression and summation order as gather_rows_kernel.  idx is not changed and the
+// other entries of dist are left as they are; sort_rows_kernel sorts after the last
+// block.  k <= 32.
+__global__ void gather_pairs_kernel(const float* __restrict__ X, const float* __restrict__ sq, int dd,
+                                    const int32_t* __restrict__ idx, float* __restrict__ dist, int k, int64_t r0,
+                                    int64_t r1) {
+  extern __shared__ float xs_all[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
+  if (row >= r1) return;
+  const int my_j = lane < k ? idx[row * k + lane] : 0;
+  const int64_t later = my_j > row ? (int64_t)my_j : row;
+  unsigned todo = __ballot_sync(0xffffffffu, lane < k && later >= r0 && later < r1);
+  if (!todo) return;
+  float* xs = xs_all + warp * dd;
+  for (int t = lane; t < dd; t += 32) xs[t] = X[row * dd + t];
+  __syncwarp();
+  const float sqi = sq[row];
+  while (todo) {  // up to four positions per step, in ascending order (warp-uniform)
+    int pos[4], c[4];
+    int cnt = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      pos[u] = todo ? __ffs(todo) - 1 : 0;
+      if (todo) {
+        todo &= todo - 1;
+        ++cnt;
+      }
+      c[u] = __shfl_sync(0xffffffffu, my_j, pos[u]);
+    }
+    float dots[4];
+    dot4<float>(X, xs, dd, c, cnt, lane, dots);
+    for (int u = 0; u < cnt; ++u)
+      if (lane == pos[u]) dist[row * k + lane] = d2_from_dot(sqi, sq[c[u]], dots[u], false);
+  }
+}
+
+// Each row of (dist, idx) sorted by (distance, id), k <= 32 entries, one warp per row.
+__global__ void sort_rows_kernel(int32_t* __restrict__ idx, float* __restrict__ dist, int64_t n, int k) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * kWarps + warp;
+  if (row >= n) return;
+  float d = lane < k ? dist[row * k + lane] : kBig;
+  int i = lane < k ? idx[row * k + lane] : 0x7fffffff;
+  warp_sort_keys(d, i, lane);
+  if (lane < k) {
+    idx[row * k + lane] = i;
+    dist[row * k + lane] = d;
+  }
+}
+
 // ---- reverse candidates ----------------------------------------------------------
 __global__ void indegree_kernel(const int32_t* __restrict__ idx, int64_t m, int32_t* __restrict__ deg) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (int64_t)gridDim.x * blockDim.x)
@@ -1065,6 +1119,46 @@ extern "C" int umapb_nnd_gather(const float* X, const float* sq, int64_t n, int3
   nnd::gather_rows_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, smem,
                             reinterpret_cast<cudaStream_t>(stream_)>>>(X, sq, n, dd, idx, dist, k, sort_rows);
   UMAPB_LAUNCH_CHECK("nnd_gather kernel");
+  count_launches(1);
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_gather_pairs(const float* X, const float* sq, int64_t n, int32_t dd, const int32_t* idx,
+                                      float* dist, int32_t k, int64_t r0, int64_t r1, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(X && sq && idx && dist, "nnd_gather_pairs: null array argument");
+  UMAPB_REQUIRE(n >= 1 && dd >= 1 && k >= 1 && k <= 32, "nnd_gather_pairs: need n >= 1, dd >= 1, 1 <= k <= 32");
+  UMAPB_REQUIRE(0 <= r0 && r0 <= r1 && r1 <= n, "nnd_gather_pairs: need 0 <= r0 <= r1 <= n");
+  const size_t smem = (size_t)nnd::kWarps * dd * sizeof(float);
+  UMAPB_REQUIRE(smem <= 200 * 1024, "nnd_gather_pairs: row dimension too large");
+  if (r1 == r0) return UMAPB_OK;
+  {
+    static std::mutex mu;
+    static bool attr[64] = {false};
+    int dev = 0;
+    UMAPB_CUDA_TRY(cudaGetDevice(&dev), "nnd_gather_pairs: device");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+      UMAPB_CUDA_TRY(cudaFuncSetAttribute(nnd::gather_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          200 * 1024),
+                     "nnd_gather_pairs: smem attribute");
+      attr[dev] = true;
+    }
+  }
+  nnd::gather_pairs_kernel<<<(unsigned)ceil_div(r1, nnd::kWarps), nnd::kWarps * 32, smem,
+                             reinterpret_cast<cudaStream_t>(stream_)>>>(X, sq, dd, idx, dist, k, r0, r1);
+  UMAPB_LAUNCH_CHECK("nnd_gather_pairs kernel");
+  count_launches(1);
+  return UMAPB_OK;
+}
+
+extern "C" int umapb_nnd_sort_rows(int32_t* idx, float* dist, int64_t n, int32_t k, umapb_stream_t stream_) {
+  clear_error();
+  UMAPB_REQUIRE(idx && dist, "nnd_sort_rows: null array argument");
+  UMAPB_REQUIRE(n >= 1 && k >= 1 && k <= 32, "nnd_sort_rows: need n >= 1 and 1 <= k <= 32");
+  nnd::sort_rows_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0,
+                          reinterpret_cast<cudaStream_t>(stream_)>>>(idx, dist, n, k);
+  UMAPB_LAUNCH_CHECK("nnd_sort_rows kernel");
   count_launches(1);
   return UMAPB_OK;
 }

@@ -320,3 +320,34 @@ def test_nndescent_k_above_the_envelope_is_rejected():
 
     with pytest.raises(ValueError, match="k <= 100"):
         NNDescent(k=101).build(np.zeros((200, 4), dtype=np.float32))
+
+
+@pytest.mark.parametrize("n,d,k,blocks", [(3001, 64, 15, 8), (1000, 36, 32, 3), (257, 784, 5, 1), (500, 20, 10, 7)])
+def test_pair_gathers_by_row_block_equal_the_gather(n, d, k, blocks):
+    """umapb_nnd_gather_pairs once per row block (the pairs whose later row is in it)
+    and then umapb_nnd_sort_rows give exactly what the one-shot gather with its row sort
+    gives: the same pair values, bit for bit, and the same order."""
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(n + k)
+    X = torch.from_numpy(rng.standard_normal((n, d)).astype(np.float32)).cuda()
+    idx0 = rng.integers(0, n, (n, k)).astype(np.int32)
+    idx0[0, :] = 0  # a row that lists itself
+    idx0[1, : k // 2] = 7  # repeated neighbours
+    s = _lib.stream_handle()
+    sq = torch.empty(n, dtype=torch.float32, device="cuda")
+    _lib.call("umapb_nnd_sqnorms", _lib.ptr(X), n, d, 0, _lib.ptr(sq), s)
+    ia = torch.from_numpy(idx0).cuda()
+    da = torch.full((n, k), -1.0, device="cuda")
+    _lib.call("umapb_nnd_gather", _lib.ptr(X), _lib.ptr(sq), n, d, _lib.ptr(ia), _lib.ptr(da), k, 1, s)
+    ib = torch.from_numpy(idx0).cuda()
+    db = torch.full((n, k), -1.0, device="cuda")
+    cuts = np.linspace(0, n, blocks + 1).astype(int)
+    cuts[1:-1] += rng.integers(-3, 4, blocks - 1)  # uneven blocks
+    for r0, r1 in zip(cuts[:-1], cuts[1:]):
+        _lib.call("umapb_nnd_gather_pairs", _lib.ptr(X), _lib.ptr(sq), n, d, _lib.ptr(ib), _lib.ptr(db), k,
+                  int(r0), int(r1), s)
+    assert bool((db >= 0).all())  # every pair was computed once the last block arrived
+    _lib.call("umapb_nnd_sort_rows", _lib.ptr(ib), _lib.ptr(db), n, k, s)
+    assert np.array_equal(ia.cpu().numpy(), ib.cpu().numpy())
+    assert np.array_equal(da.cpu().numpy().view(np.int32), db.cpu().numpy().view(np.int32))
