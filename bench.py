@@ -65,11 +65,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the untimed brute-kNN and learned-init records of the fit line")
-    ap.add_argument("--case", choices=["fit", "learned_init", "scale", "nndescent", "knn_brute", "layout",
-                                       "encoder"], default="fit",
+    ap.add_argument("--case", choices=["fit", "learned_init", "scale", "nndescent", "nndescent_1m", "knn_brute",
+                                       "layout", "encoder"], default="fit",
                     help="fit: the benchmark line; learned_init: epochs-to-trustworthiness of the learned warm start; "
                          "scale: the 1,000,000 x 128 configuration (plain fit, learned vs plain init); "
-                         "nndescent / knn_brute / layout: one untimed run of that stage (profiler captures)")
+                         "nndescent / knn_brute / layout: one untimed run of that stage (profiler captures); "
+                         "nndescent_1m: one untimed NNDescent build on the 1,000,000 x 128 configuration")
     return ap.parse_args()
 
 
@@ -748,6 +749,15 @@ def run_stage(args):
         idx, d2 = _lib.knn_brute(Xd, K_NN, extra=16)
         torch.cuda.synchronize()
         return {"case": "knn_brute", "n": 20000, "d": D, "k": K_NN, "launches": _lib.kernel_launches()}
+    if args.case == "nndescent_1m":
+        from mlx_vis_b200.datasets import anisotropic_mixture
+
+        Xs = torch.from_numpy(anisotropic_mixture(1_000_000, 128, 100, seed=0, param_seed=0)).cuda()
+        nn = NNDescent(k=K_NN, random_state=0)
+        nn.build_device(Xs)
+        torch.cuda.synchronize()
+        return {"case": "nndescent_1m", "n": 1_000_000, "d": 128, "iterations": len(nn.history_),
+                "launches": _lib.kernel_launches()}
     Xd = torch.from_numpy(make_data(args.n)).cuda()
     if args.case == "nndescent":
         nn = NNDescent(k=K_NN, random_state=0)
