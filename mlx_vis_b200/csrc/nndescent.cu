@@ -279,35 +279,19 @@ __global__ void bucket_fill_kernel(const int32_t* __restrict__ idx, int64_t m, i
 // Bucket entries hold the source row shifted left by `shift` bits (0 for the
 // reverse buckets, 5 for the join's (row, position) entries); deg == nullptr
 // takes the bucket sizes from the offsets (off[n] = total).
-__global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const int32_t* __restrict__ off,
-                                     const int32_t* __restrict__ deg, int64_t n, int k, int shift,
-                                     int32_t* __restrict__ rev) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t j = (int64_t)blockIdx.x * kWarps + warp;
-  if (j >= n) return;
-  const int cnt = deg ? deg[j] : off[j + 1] - off[j];
-  const int32_t* b = bucket + off[j];
-  if (cnt <= 32 && k <= 32) {  // the common case (mean in-degree k): one warp-wide bitonic sort
-    int v = lane < cnt ? (b[lane] >> shift) : 0x7fffffff;
-    for (int size = 2; size <= 32; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const int o = __shfl_xor_sync(0xffffffffu, v, stride);
-        const bool lower = (lane & stride) == 0, asc = (lane & size) == 0;
-        v = (lower == asc) ? min(v, o) : max(v, o);
-      }
-    }
-    if (lane < k) rev[j * k + lane] = lane < cnt ? v : 0;  // lane p holds the p-th smallest
-    return;
-  }
-  // The sorted multiset of j's sources, first k of it: each pass emits the previous
-  // source again while it has unused copies (a row that lists j twice), else the
-  // next larger source; once the bucket is exhausted the remaining slots stay 0,
-  // as the reference's scatter into zeros leaves them.
+//
+// A bucket of more than 32 entries (or k > 32), one warp: the sorted multiset of j's
+// sources, first k of it.  Each pass emits the previous source again while it has
+// unused copies (a row that lists j twice), else the next larger source; once the
+// bucket is exhausted the remaining slots stay 0, as the reference's scatter into
+// zeros leaves them.
+__device__ void bucket_select_long(const int32_t* __restrict__ b, int cnt, int k, int shift,
+                                   int32_t* __restrict__ out, int lane) {
   int prev = -1, used = 0, copies = 0;
   for (int p = 0; p < k; ++p) {
-    int out;
+    int o;
     if (prev >= 0 && used < copies) {
-      out = prev;
+      o = prev;
       ++used;
     } else {
       int best = 0x7fffffff;
@@ -316,21 +300,71 @@ __global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const i
         if (s > prev && s < best) best = s;
       }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
+      for (int q = 16; q > 0; q >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, q));
       if (best == 0x7fffffff) {
-        for (int q = p + lane; q < k; q += 32) rev[j * k + q] = 0;
+        for (int q = p + lane; q < k; q += 32) out[q] = 0;
         return;
       }
       int c = 0;
       for (int t = lane; t < cnt; t += 32) c += (b[t] >> shift) == best ? 1 : 0;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-      out = best;
+      for (int q = 16; q > 0; q >>= 1) c += __shfl_xor_sync(0xffffffffu, c, q);
+      o = best;
       prev = best;
       copies = c;
       used = 1;
     }
-    if (lane == 0) rev[j * k + p] = out;
+    if (lane == 0) out[p] = o;
+  }
+}
+
+// kSelRows consecutive rows per warp: their offsets come in one load per lane and
+// their bucket entries (up to 32 each) in kSelRows loads issued together, so a warp
+// waits for two round trips per kSelRows rows instead of per row.  A bucket of at
+// most 32 entries (the common case: the mean in-degree is k) is sorted across the
+// warp by a bitonic network; lane p then holds the p-th smallest source.
+constexpr int kSelRows = 4;
+__global__ void bucket_select_kernel(const int32_t* __restrict__ bucket, const int32_t* __restrict__ off,
+                                     const int32_t* __restrict__ deg, int64_t n, int k, int shift,
+                                     int32_t* __restrict__ rev) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j0 = ((int64_t)blockIdx.x * kWarps + warp) * kSelRows;
+  if (j0 >= n) return;
+  // lane r < kSelRows: off[j0 + r] (and deg); without deg lane kSelRows also loads the
+  // next row's offset (off[n] is the total there)
+  const int64_t jl = j0 + lane;
+  const int span = deg ? kSelRows : kSelRows + 1;
+  const int64_t lim = deg ? n : n + 1;
+  const int o = (lane < span && jl < lim) ? off[jl] : 0;
+  const int dg = (deg && lane < kSelRows && jl < n) ? deg[jl] : 0;
+  int start[kSelRows], cnt[kSelRows], v[kSelRows];
+#pragma unroll
+  for (int r = 0; r < kSelRows; ++r) {
+    start[r] = __shfl_sync(0xffffffffu, o, r);
+    const int nxt = __shfl_sync(0xffffffffu, o, r + 1);
+    const int c = deg ? __shfl_sync(0xffffffffu, dg, r) : nxt - start[r];
+    cnt[r] = j0 + r < n ? c : -1;  // -1: past the last row
+  }
+#pragma unroll
+  for (int r = 0; r < kSelRows; ++r)
+    v[r] = (cnt[r] >= 0 && cnt[r] <= 32 && lane < cnt[r]) ? (bucket[start[r] + lane] >> shift) : 0x7fffffff;
+#pragma unroll
+  for (int r = 0; r < kSelRows; ++r) {
+    if (cnt[r] < 0) break;  // warp-uniform: every lane holds the same counts
+    const int64_t j = j0 + r;
+    if (cnt[r] <= 32 && k <= 32) {
+      int x = v[r];
+      for (int size = 2; size <= 32; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          const int y = __shfl_xor_sync(0xffffffffu, x, stride);
+          const bool lower = (lane & stride) == 0, asc = (lane & size) == 0;
+          x = (lower == asc) ? min(x, y) : max(x, y);
+        }
+      }
+      if (lane < k) rev[j * k + lane] = lane < cnt[r] ? x : 0;
+    } else {
+      bucket_select_long(bucket + start[r], cnt[r], k, shift, rev + j * k, lane);
+    }
   }
 }
 
@@ -801,7 +835,7 @@ struct IterArgs {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kWarps * 32, 8) iter_kernel(IterArgs a) {
+__global__ void __launch_bounds__(kWarps * 32, 10) iter_kernel(IterArgs a) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t slot = (int64_t)blockIdx.x * kWarps + warp;
@@ -1202,8 +1236,8 @@ extern "C" int umapb_nnd_reverse(const int32_t* idx, int64_t n, int32_t k, int32
                  "nnd_reverse: degree copy");
   scan_exclusive(off, n, total, total + 8, stream);
   nnd::bucket_fill_kernel<<<blocks, 256, 0, stream>>>(idx, m, k, off, fill, bucket);
-  nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(bucket, off, deg,
-                                                                                                  n, k, 0, rev);
+  nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps * nnd::kSelRows), nnd::kWarps * 32, 0, stream>>>(
+      bucket, off, deg, n, k, 0, rev);
   UMAPB_LAUNCH_CHECK("nnd_reverse kernels");
   count_launches(4);
   return UMAPB_OK;
@@ -1270,8 +1304,8 @@ static int join_impl(const void* Xd, const float* sqd, int32_t dd, int32_t ldx, 
   scan_exclusive(off, n + 1, total, total + 8, stream);
   nnd::src_fill_kernel<<<blocks, 256, 0, stream>>>(idx_old, srcs, n, k, mc, off, fill, entries);
   if (rev_out) {  // with mc == k the buckets are the reverse-candidate buckets
-    nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps), nnd::kWarps * 32, 0, stream>>>(
-        entries, off, nullptr, n, k, 5, rev_out);
+    nnd::bucket_select_kernel<<<(unsigned)ceil_div(n, nnd::kWarps * nnd::kSelRows), nnd::kWarps * 32, 0,
+                                stream>>>(entries, off, nullptr, n, k, 5, rev_out);
   }
   const unsigned sblocks = (unsigned)ceil_div(n, 256);
   UMAPB_CUDA_TRY(cudaMemsetAsync(choff + n, 0, sizeof(int32_t), stream), "nnd_join: reset");
