@@ -135,14 +135,18 @@ class NNDescent:
         return self.neighbor_graph
 
     # ------------------------------------------------------------------
-    def build_device(self, X: torch.Tensor, x_ready=None, x_blocks=None):
+    def build_device(self, X: torch.Tensor, x_ready=None, x_blocks=None, while_first_iteration=None):
         """Device version of build: (idx int32, Euclidean dist float32) CUDA tensors.
 
         ``x_ready``: an event that X's upload records (see _device.upload_async);
         the random start, which does not read X, runs before the wait on it.
         ``x_blocks``: [(row_end, event), ...] of an upload in row blocks
         (_device.upload_blocks_async): the per-row preparation of a block then
-        starts as soon as its rows have arrived."""
+        starts as soon as its rows have arrived.
+        ``while_first_iteration``: a host function called once the first iteration's
+        kernels are enqueued and before the host waits for its change count, so that
+        its own host work (and the launches it makes on the current stream, which run
+        after that iteration) overlaps the iteration on the device."""
         if not isinstance(X, torch.Tensor) or not X.is_cuda:
             X = to_device_f32(X)
             x_ready, x_blocks = None, None
@@ -329,6 +333,8 @@ class NNDescent:
                     fp32_due = True
                 info = dict(path="full", mc_new=mc_nn, j_nn=j_nn, use_rev=use_rev, use_half=use_half, space=dd,
                             elem=2 if use_half else 4, join=join)
+            if it == 0 and while_first_iteration is not None:
+                while_first_iteration()
             n_changed, n_evals = counters[it].tolist()  # the one host read per iteration
             update_frac = n_changed / (n * k)
             idx, idx2 = idx2, idx

@@ -115,7 +115,16 @@ class UMAP:
         if n < 2:
             raise ValueError("UMAP needs at least 2 samples")
         seed = self.random_state if self.random_state is not None else _random_seed()
-        draws = self._spectral_draws(n, seed, dev) if self.init == "spectral" else None
+        # the spectral init's draws: while a host X is on its way, or (X already on the
+        # device, NNDescent) while NNDescent's first iteration runs, where their host
+        # work would otherwise leave the device idle
+        from mlx_vis_b200._knn import resolve_method
+
+        draws = None
+        defer_draws = (self.init == "spectral" and not x_blocks and self.pca_dim is None
+                       and resolve_method(self.knn_method, n) == "nndescent")
+        if self.init == "spectral" and not defer_draws:
+            draws = self._spectral_draws(n, seed, dev)
         ev.mark("upload")
 
         if self.pca_dim is not None and dim > self.pca_dim:
@@ -126,7 +135,7 @@ class UMAP:
 
         if self.verbose:
             print("Computing nearest neighbors...")
-        from mlx_vis_b200._knn import RERANK_EXTRA, resolve_method
+        from mlx_vis_b200._knn import RERANK_EXTRA
         from mlx_vis_b200._nndescent.nndescent import NNDescent
 
         k = min(self.n_neighbors, n - 1)
@@ -134,7 +143,14 @@ class UMAP:
             nn = NNDescent(k=k, verbose=self.verbose,
                            random_state=self.random_state if self.random_state is not None else 42)
             nn.profile_kernels = self.profile_kernels
-            knn_idx, knn_dist = nn.build_device(Xd, x_ready=x_ready, x_blocks=x_blocks)
+            hook = None
+            if defer_draws:
+                def hook():
+                    nonlocal draws
+                    draws = self._spectral_draws(n, seed, dev)
+            knn_idx, knn_dist = nn.build_device(Xd, x_ready=x_ready, x_blocks=x_blocks, while_first_iteration=hook)
+            if defer_draws and draws is None:  # a build that ran no iteration
+                draws = self._spectral_draws(n, seed, dev)
             x_ready = None
             self.nndescent_ = nn
         else:
