@@ -28,6 +28,7 @@ count that drives the control flow, as in the reference.
 
 from __future__ import annotations
 
+import ctypes as _c
 import os
 import time
 
@@ -252,18 +253,34 @@ class NNDescent:
         # (nndescent.py:376-378): a following full FP32 iteration takes them from its
         # join (every list position is a source there), anything else from a gather
         fp32_due = False
+        # the loop's kernel arguments: device addresses looked up once per tensor (the
+        # cache keeps each tensor alive, so an id is never reused for another one), and
+        # the counters of iteration it at byte offset 16 it, so that the host work
+        # between an iteration's count read and the next launches stays small
+        cbase = counters.data_ptr()
+        pcache = {}
+
+        def P(t):
+            if t is None:
+                return _c.c_void_p(0)
+            e = pcache.get(id(t))
+            if e is None:
+                e = pcache[id(t)] = (t, ptr(t))
+            return e[1]
+
         for it in range(self.n_iters):
             mc_nn, j_nn, mc_conv = iteration_params(update_frac, k, mc)
             use_rev = update_frac >= 0.10
-            changed, evals = counters[it, 0:1], counters[it, 1:2]
+            changed_p = _c.c_void_p(cbase + 16 * it)  # counters[it, 0] and counters[it, 1]
+            evals_p = _c.c_void_p(cbase + 16 * it + 8)
             ev = self._events()
             if update_frac < 0.5:
                 # converging path: FP32, full dimension, stored distances
                 if fp32_due:
-                    call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 0, s)
+                    call("umapb_nnd_gather", P(X), P(sq), n, d, P(idx), P(dist), k, 0, s)
                     fp32_due = False
                 if use_rev:
-                    call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
+                    call("umapb_nnd_reverse", P(idx), n, k, P(rev), P(rev_ws), rev_ws.numel(), s)
                 # the nn-of-nn distances of the NEW-first sources from the blocked join
                 join = join_on and k <= JOIN_MAX_K and mc_conv > 0 and j_nn > 0 and d % 4 == 0
                 if join and nnbuf is None:
@@ -272,11 +289,11 @@ class NNDescent:
                     join_ws = _lib.workspace(query("umapb_nnd_join_workspace", n, k, k), dev)
                 ev[0].record() if ev else None
                 if join:
-                    call("umapb_nnd_join_new", ptr(X), ptr(sq), d, ptr(idx), ptr(flags), ptr(order), n, k, mc_conv,
-                         j_nn, ptr(nnbuf), ptr(evals), ptr(join_ws), join_ws.numel(), s)
-                call("umapb_nnd_iteration", ptr(X), ptr(sq), d, d, 0, ptr(idx), ptr(dist), ptr(flags),
-                     ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None), ptr(None), n, k,
-                     mc_conv, j_nn, 1, 0, ptr(idx2), ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
+                    call("umapb_nnd_join_new", P(X), P(sq), d, P(idx), P(flags), P(order), n, k, mc_conv,
+                         j_nn, P(nnbuf), evals_p, P(join_ws), join_ws.numel(), s)
+                call("umapb_nnd_iteration", P(X), P(sq), d, d, 0, P(idx), P(dist), P(flags),
+                     P(rev if use_rev else None), P(order), P(nnbuf if join else None), P(None), n, k,
+                     mc_conv, j_nn, 1, 0, P(idx2), P(dist2), P(flags2), changed_p, evals_p, s)
                 ev[1].record() if ev else None
                 info = dict(path="converging", mc_new=mc_conv, j_nn=j_nn, use_rev=use_rev, space=d, elem=4,
                             join=join)
@@ -293,7 +310,7 @@ class NNDescent:
                 if fp32_due:
                     if not (Xd is X and not use_half and join_on and k <= JOIN_MAX_K and mc_nn == k
                             and d % 4 == 0):
-                        call("umapb_nnd_gather", ptr(X), ptr(sq), n, d, ptr(idx), ptr(dist), k, 0, s)
+                        call("umapb_nnd_gather", P(X), P(sq), n, d, P(idx), P(dist), k, 0, s)
                     else:
                         recompute = True  # the join's current-neighbour distances (curd)
                     fp32_due = False
@@ -306,7 +323,7 @@ class NNDescent:
                         src = X300h
                     else:
                         src = torch.empty((n, ldx), dtype=torch.float16, device=dev)
-                        call("umapb_nnd_to_half", ptr(Xd), n, dd, ldx, ptr(src), s)
+                        call("umapb_nnd_to_half", P(Xd), n, dd, ldx, P(src), s)
                 else:
                     src = Xd
                 join = join_on and k <= JOIN_MAX_K and mc_nn > 0 and (use_half or dd % 4 == 0)
@@ -318,16 +335,16 @@ class NNDescent:
                 # buckets are the reverse-candidate buckets: it writes rev itself
                 rev_in_join = join and use_rev and mc_nn == k
                 if use_rev and not rev_in_join:
-                    call("umapb_nnd_reverse", ptr(idx), n, k, ptr(rev), ptr(rev_ws), rev_ws.numel(), s)
+                    call("umapb_nnd_reverse", P(idx), n, k, P(rev), P(rev_ws), rev_ws.numel(), s)
                 ev[0].record() if ev else None
                 if join:
-                    call("umapb_nnd_join", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(order), n, k,
-                         mc_nn, j_nn, ptr(nnbuf), ptr(curd), ptr(rev if rev_in_join else None), ptr(evals),
-                         ptr(join_ws), join_ws.numel(), s)
-                call("umapb_nnd_iteration", ptr(src), ptr(sqd), dd, ldx, int(use_half), ptr(idx), ptr(dist), ptr(None),
-                     ptr(rev if use_rev else None), ptr(order), ptr(nnbuf if join else None),
-                     ptr(curd if join else None), n, k, mc_nn, j_nn, 0, int(recompute), ptr(idx2),
-                     ptr(dist2), ptr(flags2), ptr(changed), ptr(evals), s)
+                    call("umapb_nnd_join", P(src), P(sqd), dd, ldx, int(use_half), P(idx), P(order), n, k,
+                         mc_nn, j_nn, P(nnbuf), P(curd), P(rev if rev_in_join else None), evals_p,
+                         P(join_ws), join_ws.numel(), s)
+                call("umapb_nnd_iteration", P(src), P(sqd), dd, ldx, int(use_half), P(idx), P(dist), P(None),
+                     P(rev if use_rev else None), P(order), P(nnbuf if join else None),
+                     P(curd if join else None), n, k, mc_nn, j_nn, 0, int(recompute), P(idx2),
+                     P(dist2), P(flags2), changed_p, evals_p, s)
                 ev[1].record() if ev else None
                 if it == 4:  # FP32 recompute after the last FP16 iteration (nndescent.py:376-378)
                     fp32_due = True
