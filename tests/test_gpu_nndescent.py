@@ -76,6 +76,28 @@ def test_nndescent_reverse_candidates_match_oracle():
     assert np.array_equal(rev.cpu().numpy(), want)
 
 
+@pytest.mark.parametrize("n,k", [(1003, 15), (37, 5), (2, 1)])
+def test_nndescent_reverse_candidates_ragged_rows_and_hubs(n, k):
+    """The reverse-bucket select works on groups of 4 rows: a last group with fewer
+    rows and groups that mix buckets of more than 32 entries (hubs) with short ones."""
+    import torch
+
+    from mlx_vis_b200 import _lib
+
+    rng = np.random.default_rng(n + k)
+    idx = rng.integers(0, n, size=(n, k)).astype(np.int32)
+    hubs = min(3, n - 1) + 1
+    idx[: n // 2, 0] = rng.integers(0, hubs, size=n // 2)  # rows 0..hubs-1 become hubs
+    want = onnd.reverse_candidates(idx)
+    d_idx = torch.from_numpy(idx).cuda()
+    rev = torch.full_like(d_idx, -7)
+    ws = _lib.workspace(_lib.query("umapb_nnd_reverse_workspace", n, k), d_idx.device)
+    _lib.call("umapb_nnd_reverse", _lib.ptr(d_idx), n, k, _lib.ptr(rev), _lib.ptr(ws), ws.numel(),
+              _lib.stream_handle())
+    got = rev.cpu().numpy()
+    assert np.array_equal(got, want)
+
+
 def test_nndescent_small_and_edge_cases():
     from mlx_vis_b200 import NNDescent
 
